@@ -1,0 +1,213 @@
+/*
+ * sma.h -- C ABI of libsma, the B200 (sm_100a) implementation of the two solve-free
+ * interior eigensolvers of MathiasTensor/sparse_matrix_algorithms:
+ *
+ *   chebyshev_poly_real_symm_sparse(A, emin, emax; ...)    chebyshev_subspace_iteration.jl:667
+ *   chebyshev_poly_real_symm_sparse(matvec!, n, emin, emax; ...)   chebyshev_subspace_iteration.jl:771
+ *   polfed(A::MatrixFreeRealSymOp, nev, degree; ...)        polfed.jl:1128
+ *   polfed(matvec!, n, nev, degree; matblock!=nothing, ...) polfed.jl:1183
+ *
+ * Every entry point takes plain pointers and sizes.  Unless stated otherwise pointers
+ * are HOST pointers.  Dense blocks handed to the device entry points (suffix _dev) are
+ * ROW-MAJOR: element (i, j) of an n x b block with leading dimension ld sits at
+ * X[i*ld + j] (ld >= b).  Blocks exchanged with host callers are column-major, as a
+ * Julia Matrix{Float64} is.
+ *
+ * Status codes mirror the reference's error behaviour: SMA_ERR_ARG is Julia's
+ * ArgumentError, SMA_ERR_BOUNDS the `error(...)` of polfed.jl:1130, SMA_ERR_WINDOW the
+ * unknown-window error of polfed.jl:413.  sma_last_error() returns the message of the
+ * calling thread's last failure.
+ *
+ * Threading: a context owns one CUDA stream and its library handles; use a context
+ * from one host thread at a time.  Different contexts are independent.
+ */
+#ifndef SMA_H
+#define SMA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SMA_ABI_VERSION 1
+
+enum sma_status {
+  SMA_OK = 0,
+  SMA_ERR_ARG = 1,          /* ArgumentError (chebyshev_subspace_iteration.jl:669-674) */
+  SMA_ERR_NONSYMMETRIC = 2, /* issymmetric(Ain) failed (chebyshev_subspace_iteration.jl:669) */
+  SMA_ERR_INTERVAL = 3,     /* mapped interval not inside [-1,1] (chebyshev_subspace_iteration.jl:689) */
+  SMA_ERR_CUDA = 4,         /* CUDA / cuBLAS / cuSOLVER failure */
+  SMA_ERR_TIMEOUT = 5,      /* a bounded device wait gave up */
+  SMA_ERR_NOCONV = 6,
+  SMA_ERR_NOMEM = 7,
+  SMA_ERR_BOUNDS = 8,       /* "Matrix-free POLFED requires spectral bounds" (polfed.jl:1130) */
+  SMA_ERR_WINDOW = 9,       /* "Unknown window type" (polfed.jl:413) */
+  SMA_ERR_CALLBACK = 10,    /* a user operator callback returned non-zero */
+  SMA_ERR_INTERNAL = 11
+};
+
+enum sma_window { SMA_WINDOW_STEP = 0, SMA_WINDOW_DELTA = 1, SMA_WINDOW_SMOOTH = 2 };
+
+/* Arithmetic of the block Clenshaw filter.  FP64 is the reference's arithmetic. */
+enum sma_precision { SMA_PREC_FP64 = 0, SMA_PREC_FP32 = 1 };
+
+typedef struct sma_ctx sma_ctx;
+typedef struct sma_op sma_op;
+typedef struct sma_result sma_result;
+
+/* Device block operator supplied by the caller (the GPU form of the reference's
+ * matblock!, chebyshev_subspace_iteration.jl:186-197 / polfed.jl:209-219): write
+ * Y = A X for the row-major n x b blocks X_dev, Y_dev (leading dimension ld, FP64),
+ * enqueuing all work on `stream` (a cudaStream_t).  Return 0 on success. */
+typedef int (*sma_matblock_fn)(void *user, const double *X_dev, double *Y_dev, int64_t n,
+                               int64_t b, int64_t ld, void *stream);
+
+/* Keyword arguments of chebyshev_poly_real_symm_sparse (chebyshev_subspace_iteration.jl:667). */
+typedef struct sma_cheb_opts {
+  double smin, smax;      /* spectral bounds, used when has_bounds != 0 */
+  int64_t has_bounds;     /* 0: Gershgorin bounds (smin=nothing / smax=nothing) */
+  double sigma;           /* centre of the :delta window */
+  int64_t m0;             /* subspace size (default 200) */
+  int64_t degree;         /* filter degree (default 80) */
+  int64_t maxiter;        /* default 8 */
+  double tol;             /* default 1e-10 */
+  double res_gate;        /* default 1e-6 */
+  int64_t jackson;        /* default 1 */
+  int64_t debug;          /* print the per-iteration line */
+  int64_t two_hit;        /* default 1 */
+  int64_t seed;           /* start block seed (default 1) */
+  int64_t window_type;    /* enum sma_window, default SMA_WINDOW_STEP */
+  int64_t matrix_free;    /* 0: sparse overload semantics (always maxiter iterations,
+                             chebyshev_subspace_iteration.jl:731-749); 1: matrix-free overload
+                             semantics (two_hit early exit, chebyshev_subspace_iteration.jl:827-836) */
+  int64_t precision;      /* enum sma_precision of the filter, default SMA_PREC_FP64 */
+  int64_t reserved[8];
+} sma_cheb_opts;
+
+/* Keyword arguments of polfed (polfed.jl:1128). */
+typedef struct sma_polfed_opts {
+  int64_t s;              /* block size (default 8) */
+  double smin, smax;      /* spectral bounds (required) */
+  int64_t has_bounds;     /* 0 -> SMA_ERR_BOUNDS, as polfed.jl:1130 */
+  double sigma;           /* default 0 */
+  double emin, emax;      /* default -Inf, +Inf */
+  double tol;             /* default 1e-10 */
+  int64_t threaded;       /* accepted, unused (as in the reference) */
+  int64_t overextract;    /* default 2 */
+  int64_t refine;         /* default 1 */
+  int64_t window_type;    /* default SMA_WINDOW_STEP */
+  int64_t jackson;        /* default 1 */
+  int64_t mmax;           /* 0: ceil(2.8*nev/s) (polfed.jl:1132) */
+  double rtol;            /* default 1e-12 */
+  int64_t reorth_passes;  /* default 1 */
+  int64_t extra_keep;     /* default 8 */
+  int64_t seed;           /* default 1 */
+  int64_t show_progress;  /* print the _progress_line summary (polfed.jl:991-1000) */
+  int64_t chunk;          /* default 64 (extraction chunking; results do not depend on it) */
+  int64_t precision;      /* enum sma_precision of the filter, default SMA_PREC_FP64 */
+  int64_t reserved[8];
+} sma_polfed_opts;
+
+/* Per-solve counters and phase timings (device time, CUDA events). */
+typedef struct sma_stats {
+  int64_t iterations;     /* Chebyshev iterations or POLFED blocks */
+  int64_t basis_dim;      /* POLFED basis dimension M; Chebyshev m0 */
+  int64_t spmm_steps;     /* block sparse products issued by the filter */
+  int64_t spmm_columns;   /* sum over those products of the block width */
+  double filter_ms;       /* block Clenshaw filter */
+  double orth_ms;         /* orthogonalization / reorthogonalization */
+  double rr_ms;           /* Rayleigh-Ritz, residuals, extraction */
+  double total_ms;        /* whole solve, wall clock from call to return */
+  double filter_bytes;    /* algorithmic bytes of the filter's sparse products */
+  int64_t qr_fallbacks;   /* blocks that left CholQR2 for shifted CholQR3 / Householder */
+  int64_t warnings;       /* bit 0: interval outside the spectral bounds */
+  int64_t reserved[8];
+} sma_stats;
+
+/* ---------------------------------------------------------------- library, context */
+int sma_abi_version(void);
+const char *sma_last_error(void);
+int sma_ctx_create(int device, sma_ctx **out);
+int sma_ctx_destroy(sma_ctx *ctx);
+int sma_ctx_synchronize(sma_ctx *ctx);
+/* The context's cudaStream_t. */
+void *sma_ctx_stream(sma_ctx *ctx);
+
+/* ---------------------------------------------------------------- operators */
+/* Upload a sparse symmetric matrix given as CSC arrays (Julia's SparseMatrixCSC
+ * colptr/rowval/nzval, chebyshev_subspace_iteration.jl:667; for a symmetric matrix
+ * these are also its CSR arrays).  index_base 1 for Julia, 0 for C.  Row indices must
+ * be sorted within each column.  check_symmetric != 0 verifies A == A^T exactly on the
+ * device (the issymmetric check of chebyshev_subspace_iteration.jl:669). */
+int sma_op_create_csc(sma_ctx *ctx, int64_t n, int64_t nnz, const int64_t *colptr,
+                      const int64_t *rowval, const double *nzval, int64_t index_base,
+                      int64_t check_symmetric, sma_op **out);
+/* Matrix-free 1D Laplacian tridiag(-1,2,-1) as a device stencil (the reference's
+ * lap1d_matblock!, polfed.jl:1209-1219). */
+int sma_op_create_lap1d(sma_ctx *ctx, int64_t n, sma_op **out);
+/* Matrix-free operator from a caller-supplied device block callback
+ * (MatrixFreeRealSymOp(n, matvec!, matblock!), polfed.jl:165). */
+int sma_op_create_matblock(sma_ctx *ctx, int64_t n, sma_matblock_fn fn, void *user,
+                           sma_op **out);
+int sma_op_destroy(sma_op *op);
+int sma_op_info(const sma_op *op, int64_t *n, int64_t *nnz);
+/* Gershgorin bounds (chebyshev_subspace_iteration.jl:351-367); explicit matrices only. */
+int sma_gershgorin_bounds(sma_op *op, double *smin, double *smax);
+
+/* ---------------------------------------------------------------- filter coefficients */
+/* jackson_kernel(K): g[0..K] (chebyshev_subspace_iteration.jl:376-387). */
+int sma_jackson_kernel(int64_t K, double *g);
+/* cheb_delta_coeffs (chebyshev_subspace_iteration.jl:400-414). */
+int sma_cheb_delta_coeffs(double sigma_hat, int64_t K, int64_t jackson, double *c);
+/* cheb_window_coeffs (chebyshev_subspace_iteration.jl:430-447). */
+int sma_cheb_window_coeffs(double a, double b, int64_t K, int64_t jackson, double *c);
+/* cheb_smooth_window_coeffs (chebyshev_subspace_iteration.jl:465-489). */
+int sma_cheb_smooth_window_coeffs(double a, double b, int64_t K, int64_t jackson,
+                                  int64_t nsamp, double delta, double *c);
+/* _build_coeffs (polfed.jl:404-414): c has degree+1 entries. */
+int sma_build_coeffs(int64_t degree, double smin, double smax, double sigma, double emin,
+                     double emax, int64_t window_type, int64_t jackson, double *c);
+
+/* ---------------------------------------------------------------- the hot path */
+/* Y = p(A_hat) Q by the block Clenshaw recurrence (apply_poly_block!,
+ * chebyshev_subspace_iteration.jl:554-591 and 598-635, polfed.jl:464-545) on device
+ * blocks.  coeffs: K+1 host doubles.  precision selects the element type of Q_dev and
+ * Y_dev (double for SMA_PREC_FP64, float for SMA_PREC_FP32).  Synchronous. */
+int sma_apply_poly_block_dev(sma_op *op, const double *coeffs, int64_t K, double smin,
+                             double smax, const void *Q_dev, int64_t ldq, void *Y_dev,
+                             int64_t ldy, int64_t b, int64_t precision);
+/* Same filter on host column-major n x b FP64 blocks (copies in and out). */
+int sma_apply_poly_block(sma_op *op, const double *coeffs, int64_t K, double smin,
+                         double smax, const double *Q, double *Y, int64_t b,
+                         int64_t precision);
+/* Y = A X on device row-major FP64 blocks (apply_A_block!). Synchronous. */
+int sma_spmm_dev(sma_op *op, const double *X_dev, int64_t ldx, double *Y_dev, int64_t ldy,
+                 int64_t b);
+
+/* ---------------------------------------------------------------- solvers */
+void sma_cheb_opts_default(sma_cheb_opts *o);
+void sma_polfed_opts_default(sma_polfed_opts *o);
+/* chebyshev_poly_real_symm_sparse; result sorted by eigenvalue, absolute residuals
+ * (chebyshev_subspace_iteration.jl:750-756). */
+int sma_cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts *opts,
+                   sma_result **out);
+/* polfed; result order follows polfed.jl:1148-1157 (by eigenvalue when the nev-th
+ * smallest residual is below tol, else by residual). */
+int sma_polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polfed_opts *opts,
+                     sma_result **out);
+
+/* ---------------------------------------------------------------- results */
+/* k = number of returned pairs, n = vector length. */
+int sma_result_count(const sma_result *r, int64_t *k, int64_t *n);
+/* Copy eigenvalues (k), eigenvectors (n x k, column-major) and residuals (k); any of
+ * the three pointers may be NULL. */
+int sma_result_copy(const sma_result *r, double *lam, double *X, double *res);
+int sma_result_stats(const sma_result *r, sma_stats *stats);
+int sma_result_free(sma_result *r);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SMA_H */

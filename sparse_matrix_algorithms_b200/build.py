@@ -1,0 +1,78 @@
+"""Build libsma.so in-tree for sm_100a with nvcc.
+
+``python -m sparse_matrix_algorithms_b200.build`` (or ``build_library()``) compiles
+every ``csrc/*.cu`` file to an object (in parallel) and links the shared library
+``sparse_matrix_algorithms_b200/libsma.so`` against cuBLAS and cuSOLVER.  Objects
+are rebuilt only when a source or header is newer.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+BUILD = os.path.join(PKG, "_build")
+LIB = os.path.join(PKG, "libsma.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
+                     "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
+
+
+def _nvcc() -> str:
+    cand = os.environ.get("NVCC") or shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(cand):
+        raise RuntimeError("nvcc not found; set NVCC or put CUDA's bin directory on PATH")
+    return cand
+
+
+def _cuda_lib_dir(nvcc: str) -> str:
+    return os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(nvcc))), "lib64")
+
+
+def _headers():
+    return glob.glob(os.path.join(CSRC, "*.h")) + [os.path.join(ROOT, "include", "sma.h")]
+
+
+def build_library(verbose: bool = False, jobs: int = 0) -> str:
+    """Compile and link libsma.so; returns its path."""
+    nvcc = _nvcc()
+    os.makedirs(BUILD, exist_ok=True)
+    sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    hdr_time = max(os.path.getmtime(h) for h in _headers())
+
+    def compile_one(src):
+        obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+        if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr_time):
+            return obj
+        cmd = [nvcc] + NVCC_FLAGS + ["-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
+        return obj
+
+    with cf.ThreadPoolExecutor(max_workers=jobs or min(8, os.cpu_count() or 1)) as ex:
+        objs = list(ex.map(compile_one, sources))
+    newest = max(os.path.getmtime(o) for o in objs)
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
+        libdir = _cuda_lib_dir(nvcc)
+        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + [
+            "-L" + libdir, "-lcublas", "-lcusolver", "-Xlinker", "-rpath," + libdir]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build_library(verbose="-v" in sys.argv))

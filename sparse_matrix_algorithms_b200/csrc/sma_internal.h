@@ -1,0 +1,253 @@
+// Internal declarations shared by the libsma translation units.
+#pragma once
+
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/sma.h"
+
+namespace sma {
+
+// ------------------------------------------------------------------ errors
+// Internal code throws sma::Error; the extern "C" layer turns it into a status code
+// and the thread-local message returned by sma_last_error().
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+void set_last_error(const std::string &msg);
+
+#define SMA_CUDA(call)                                                                   \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      throw ::sma::Error(e_ == cudaErrorMemoryAllocation ? SMA_ERR_NOMEM : SMA_ERR_CUDA, \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));            \
+  } while (0)
+
+#define SMA_CUBLAS(call)                                                                 \
+  do {                                                                                   \
+    cublasStatus_t s_ = (call);                                                          \
+    if (s_ != CUBLAS_STATUS_SUCCESS)                                                     \
+      throw ::sma::Error(SMA_ERR_CUDA, std::string(#call) + ": cublas status " +        \
+                                           std::to_string((int)s_));                    \
+  } while (0)
+
+#define SMA_CUSOLVER(call)                                                               \
+  do {                                                                                   \
+    cusolverStatus_t s_ = (call);                                                        \
+    if (s_ != CUSOLVER_STATUS_SUCCESS)                                                   \
+      throw ::sma::Error(SMA_ERR_CUDA, std::string(#call) + ": cusolver status " +      \
+                                           std::to_string((int)s_));                    \
+  } while (0)
+
+#define SMA_CHECK_LAUNCH() SMA_CUDA(cudaGetLastError())
+
+inline void require(bool ok, int code, const std::string &msg) {
+  if (!ok) throw Error(code, msg);
+}
+
+}  // namespace sma
+
+// ------------------------------------------------------------------ context
+struct sma_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cublasHandle_t cublas = nullptr;
+  cusolverDnHandle_t cusolver = nullptr;
+  int num_sms = 148;
+};
+
+enum op_kind { OP_CSR = 0, OP_LAP1D = 1, OP_MATBLOCK = 2 };
+
+struct sma_op {
+  sma_ctx *ctx = nullptr;
+  int kind = OP_CSR;
+  int64_t n = 0, nnz = 0;
+  // CSR (== CSC of the symmetric matrix), 0-based, int32 indices
+  int *rowptr = nullptr;
+  int *colind = nullptr;
+  double *val64 = nullptr;
+  float *val32 = nullptr;  // created on first FP32 use
+  // Gershgorin bounds, computed on upload
+  double gersh_min = 0, gersh_max = 0;
+  bool has_gersh = false;
+  int sym_state = 0;  // 0 unknown, 1 A == A^T, 2 not symmetric
+  // caller callback
+  sma_matblock_fn fn = nullptr;
+  void *user = nullptr;
+};
+
+namespace sma {
+
+// ------------------------------------------------------------------ device buffers
+// Stream-ordered device allocation owned by one solve.
+template <typename T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t count = 0;
+  cudaStream_t stream = nullptr;
+  DevBuf() = default;
+  DevBuf(size_t n, cudaStream_t s) { alloc(n, s); }
+  void alloc(size_t n, cudaStream_t s) {
+    release();
+    stream = s;
+    count = n;
+    if (n) SMA_CUDA(cudaMallocAsync((void **)&p, n * sizeof(T), s));
+  }
+  void release() {
+    if (p) cudaFreeAsync(p, stream);
+    p = nullptr;
+    count = 0;
+  }
+  ~DevBuf() { release(); }
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  DevBuf(DevBuf &&o) noexcept : p(o.p), count(o.count), stream(o.stream) { o.p = nullptr; o.count = 0; }
+  DevBuf &operator=(DevBuf &&o) noexcept {
+    if (this != &o) { release(); p = o.p; count = o.count; stream = o.stream; o.p = nullptr; o.count = 0; }
+    return *this;
+  }
+  T *get() const { return p; }
+};
+
+// A row-major block view: element (i, j) at ptr[i*ld + j].
+template <typename T>
+struct Block {
+  T *ptr;
+  int64_t ld;
+};
+
+// ------------------------------------------------------------------ kernels (kernels.cu)
+// out = ck*Q + alpha*(A*B1) + beta*B1 - B2 over b columns (one Clenshaw step).
+// Q may be null (ck ignored), B2 may be null, has_self=false drops the beta*B1 term.
+template <typename T>
+void launch_clenshaw_step(const sma_op *op, cudaStream_t st, int64_t b, const T *Q, int64_t ldq,
+                          const T *B1, const T *B2, int64_t ldb, T *out, int64_t ldo, double ck,
+                          double alpha, double beta, bool has_self);
+// out = ck * Q
+template <typename T>
+void launch_scale_block(cudaStream_t st, int64_t n, int64_t b, const T *Q, int64_t ldq, T *out,
+                        int64_t ldo, double ck);
+// out = ck*Q + alpha*AX + beta*B1 - B2 (the matrix-free axpy of
+// chebyshev_subspace_iteration.jl:616-620); B2 may be null.
+template <typename T>
+void launch_clenshaw_axpy(cudaStream_t st, int64_t n, int64_t b, const T *Q, int64_t ldq,
+                          const T *AX, int64_t ldax, const T *B1, const T *B2, int64_t ldb,
+                          T *out, int64_t ldo, double ck, double alpha, double beta);
+
+void launch_randn(cudaStream_t st, int64_t n, int64_t m, uint64_t seed, double *out, int64_t ld);
+// Column reductions over row-major n x k blocks (deterministic two-stage sums).
+//   mode 0: out[j] = sum_i X[i,j]*Y[i,j]
+//   mode 1: out[j] = sqrt(sum_i (Y[i,j] - lam[j]*X[i,j])^2)
+void column_reduce(cudaStream_t st, int mode, int64_t n, int64_t k, const double *X, int64_t ldx,
+                   const double *Y, int64_t ldy, const double *lam, double *out,
+                   DevBuf<double> &scratch);
+// dst (row-major n x b, ldd) <- src (row-major, lds); optional type conversion
+template <typename TS, typename TD>
+void launch_copy_block(cudaStream_t st, int64_t n, int64_t b, const TS *src, int64_t lds, TD *dst,
+                       int64_t ldd);
+// dst column-major n x k (ld n) <- src row-major n x k (ld lds)
+void launch_rowmajor_to_colmajor(cudaStream_t st, int64_t n, int64_t k, const double *src,
+                                 int64_t lds, double *dst);
+void launch_colmajor_to_rowmajor(cudaStream_t st, int64_t n, int64_t k, const double *src,
+                                 double *dst, int64_t ldd);
+// H = 0.5*(G + G^T) for a k x k column-major G (ld ldg) into H (ld ldh)
+void launch_symmetrize(cudaStream_t st, int64_t k, const double *G, int64_t ldg, double *H,
+                       int64_t ldh);
+// T[o:o+r, o:o+r] = Aj ; T[o+r:o+r+r2, o:o+r] = Bj ; T[o:o+r, o+r:o+r+r2] = Bj^T
+void launch_place_blocks(cudaStream_t st, double *T, int64_t ldt, int64_t o, int64_t r,
+                         const double *Aj, int64_t lda, const double *Bj, int64_t ldbj,
+                         int64_t r2);
+// dst[:, j] = src[:, idx[j]] for column-major M x k (device idx)
+void launch_gather_columns_cm(cudaStream_t st, int64_t M, int64_t k, const double *src,
+                              int64_t lds, const int64_t *idx, double *dst, int64_t ldd);
+// dst[i, j] = src[i, idx[j]] for row-major blocks (device idx)
+void launch_gather_columns_rm(cudaStream_t st, int64_t n, int64_t k, const double *src,
+                              int64_t lds, const int64_t *idx, double *dst, int64_t ldd);
+// Gershgorin partial bounds of a CSR matrix
+void gershgorin_device(const sma_op *op, double *smin, double *smax);
+// Exact symmetry and sortedness check; returns 0 ok, 1 unsorted, 2 non-symmetric
+int check_csr_device(const sma_op *op);
+// In-place shift of the diagonal of a k x k column-major matrix
+void launch_add_diagonal(cudaStream_t st, int64_t k, double *G, int64_t ld, double shift);
+// Zero the strict lower triangle of a k x k column-major matrix
+void launch_zero_lower(cudaStream_t st, int64_t k, double *G, int64_t ld);
+
+// ------------------------------------------------------------------ host coefficient builders
+std::vector<double> jackson_kernel(int64_t K);
+std::vector<double> cheb_delta_coeffs(double sh, int64_t K, bool jackson);
+std::vector<double> cheb_window_coeffs(double a, double b, int64_t K, bool jackson);
+std::vector<double> cheb_smooth_window_coeffs(double a, double b, int64_t K, bool jackson,
+                                              int64_t nsamp, double delta);
+std::vector<double> build_coeffs(int64_t degree, double smin, double smax, double sigma,
+                                 double emin, double emax, int64_t window_type, bool jackson);
+
+// ------------------------------------------------------------------ filter (filter.cu)
+// Work space of the block Clenshaw recurrence: three n x b blocks (+ AX for matrix-free).
+template <typename T>
+struct ClenshawWork {
+  DevBuf<T> b1, b2, tmp, ax;
+  int64_t n = 0, bcap = 0;
+  void ensure(const sma_op *op, int64_t n_, int64_t b, cudaStream_t st);
+};
+
+// Y = p(A_hat) Q.  Returns the sparse block products issued and their algorithmic bytes.
+struct FilterCount {
+  int64_t steps = 0;
+  double bytes = 0.0;
+};
+template <typename T>
+FilterCount apply_poly_block(const sma_op *op, cudaStream_t st, const std::vector<double> &coeffs,
+                         double smin, double smax, const T *Q, int64_t ldq, T *Y, int64_t ldy,
+                         int64_t b, ClenshawWork<T> &work);
+
+// AX = A X for FP64 blocks (any operator kind)
+void op_apply(const sma_op *op, cudaStream_t st, const double *X, int64_t ldx, double *Y,
+              int64_t ldy, int64_t b);
+
+// Algorithmic bytes of one fused Clenshaw step over b columns
+double clenshaw_step_bytes(const sma_op *op, int64_t b, int elem_bytes);
+
+// ------------------------------------------------------------------ dense (dense.cu)
+struct Dense {
+  sma_ctx *ctx;
+  explicit Dense(sma_ctx *c) : ctx(c) {}
+  // C (col-major, m x k, ldc) = alpha * X^T Y + beta*C, X row-major n x m (ldx), Y n x k
+  void gram(int64_t n, int64_t m, int64_t k, const double *X, int64_t ldx, const double *Y,
+            int64_t ldy, double *C, int64_t ldc, double alpha = 1.0, double beta = 0.0);
+  // Y (row-major n x p, ldy) = alpha * X C + beta*Y, X row-major n x m, C col-major m x p
+  void mul_small(int64_t n, int64_t m, int64_t p, const double *X, int64_t ldx, const double *C,
+                 int64_t ldc, double *Y, int64_t ldy, double alpha, double beta, bool transC = false);
+  // Symmetric eigen-decomposition of a k x k column-major matrix in place (vectors
+  // overwrite A, eigenvalues ascending in w_dev). uplo_upper selects the triangle read.
+  void syevd(int64_t k, double *A, int64_t lda, double *w_dev, bool uplo_upper);
+};
+
+// Orthonormalize the columns of a row-major n x k block in place and return the
+// upper-triangular factor R (k x k, column-major, host) with X_in = Q R.
+// truncate: apply the reference's rank rule (keep the first count(|R_ii| > rtol*max|R_ii|)
+// columns).  Returns the kept rank.  *fallbacks is incremented when CholQR2 is not used.
+int64_t orthonormalize(sma_ctx *ctx, int64_t n, int64_t k, double *X, int64_t ldx,
+                       bool truncate, double rtol, std::vector<double> *R_out,
+                       int64_t *fallbacks);
+
+// ------------------------------------------------------------------ result
+}  // namespace sma
+
+struct sma_result {
+  int64_t n = 0, k = 0;
+  std::vector<double> lam, res;
+  double *X_dev = nullptr;  // row-major n x k (ld k), owned
+  int64_t ldx = 0;
+  sma_ctx *ctx = nullptr;
+  sma_stats stats{};
+};
