@@ -123,7 +123,9 @@ typedef struct sma_stats {
   double filter_bytes;    /* algorithmic bytes of the filter's sparse products */
   int64_t qr_fallbacks;   /* blocks that left CholQR2 for shifted CholQR3 / Householder */
   int64_t warnings;       /* bit 0: interval outside the spectral bounds */
-  int64_t reserved[8];
+  int64_t kernel_launches; /* this library's own CUDA kernels launched by the solve
+                              (cuBLAS / cuSOLVER launches not included) */
+  int64_t reserved[7];
 } sma_stats;
 
 /* ---------------------------------------------------------------- library, context */

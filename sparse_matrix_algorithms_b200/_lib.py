@@ -77,7 +77,8 @@ class Stats(ctypes.Structure):
     _fields_ = [("iterations", c_int64), ("basis_dim", c_int64), ("spmm_steps", c_int64),
                 ("spmm_columns", c_int64), ("filter_ms", c_double), ("orth_ms", c_double),
                 ("rr_ms", c_double), ("total_ms", c_double), ("filter_bytes", c_double),
-                ("qr_fallbacks", c_int64), ("warnings", c_int64), ("reserved", c_int64 * 8)]
+                ("qr_fallbacks", c_int64), ("warnings", c_int64), ("kernel_launches", c_int64),
+                ("reserved", c_int64 * 7)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}

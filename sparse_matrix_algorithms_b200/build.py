@@ -37,7 +37,8 @@ def _cuda_lib_dir(nvcc: str) -> str:
 
 
 def _headers():
-    return glob.glob(os.path.join(CSRC, "*.h")) + [os.path.join(ROOT, "include", "sma.h")]
+    return (glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh"))
+            + [os.path.join(ROOT, "include", "sma.h")])
 
 
 def build_library(verbose: bool = False, jobs: int = 0) -> str:

@@ -3,6 +3,7 @@
 // returns a status code; nothing throws across the C boundary.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <string>
 
 #include "sma_internal.h"
@@ -90,6 +91,8 @@ int sma_ctx_create(int device, sma_ctx **out) {
     DeviceGuard g(device);
     auto *ctx = new sma_ctx();
     ctx->device = device;
+    const char *at = std::getenv("SMA_AUTOTUNE");
+    ctx->autotune = !(at && std::string(at) == "0");
     try {
       SMA_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
       SMA_CUBLAS(cublasCreate(&ctx->cublas));
@@ -97,6 +100,13 @@ int sma_ctx_create(int device, sma_ctx **out) {
       SMA_CUSOLVER(cusolverDnCreate(&ctx->cusolver));
       SMA_CUSOLVER(cusolverDnSetStream(ctx->cusolver, ctx->stream));
       SMA_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
+      // Keep freed stream-ordered allocations in this process's pool: solves allocate
+      // and free their blocks every call.
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
     } catch (...) {
       if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
       if (ctx->cublas) cublasDestroy(ctx->cublas);

@@ -1,0 +1,311 @@
+// The fused CSR Clenshaw step and its online autotuner (included by csr_clenshaw_f64.cu and
+// csr_clenshaw_f32.cu, one translation unit per element type).
+//
+//   out[i, :] = ck*Q[i, :] + alpha * sum_j A[i,j] B1[j, :] + beta*B1[i, :] - B2[i, :]
+//
+// One CTA of 256 threads owns 256/G consecutive rows; a group of G threads owns one row and
+// each thread covers V consecutive columns of every G*V-wide column pass (V*sizeof(T) is
+// 8..32 bytes: one or two 16-byte loads per neighbour row).  Gathers are issued U at a
+// time so that U neighbour rows are in flight per thread, and the epilogue operands (the
+// row of Q, B1, B2) are requested before the gathers.  Two families differ in how a
+// thread obtains its row's (column, value) pairs:
+//   DIRECT  every thread reads them itself; the G lanes of a group read the same
+//           addresses, which the L1 cache serves as one broadcast;
+//   STAGED  the CTA first copies the pairs of all its rows (one contiguous CSR range)
+//           into shared memory with coalesced loads, then reads them from there.
+// Every configuration accumulates with FMA in ascending column order -- the order of the
+// reference's CSC product on a symmetric matrix -- so all configurations write
+// bit-identical results, and the autotuner may run real recurrence steps with different
+// configurations while it measures them.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+
+#include "sma_internal.h"
+#include "vec.cuh"
+
+namespace sma {
+namespace csr {
+
+constexpr int kThreads = 256;
+constexpr int kStage = 1024;  // CSR entries a STAGED CTA keeps in shared memory
+
+template <typename T, int V, bool HQ, bool HS, bool HB>
+__device__ __forceinline__ void epilogue(T *__restrict__ out, const T (&acc)[V], const T (&q)[V],
+                                         const T (&s)[V], const T (&t)[V], T ck, T alpha, T beta) {
+  T r[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    T x = alpha * acc[v];
+    if constexpr (HQ) x = ck * q[v] + x;
+    if constexpr (HS) x = x + beta * s[v];
+    if constexpr (HB) x = x - t[v];
+    r[v] = x;
+  }
+  stv<T, V>(out, r);
+}
+
+// acc += sum over the row's entries j in [start, end) of vals[j-off] * B1c[cols[j-off] * ldb]
+template <typename T, int V, int U>
+__device__ __forceinline__ void row_product(const int *__restrict__ cols, const T *__restrict__ vals,
+                                            int off, int start, int end, const T *__restrict__ B1c,
+                                            int64_t ldb, T (&acc)[V]) {
+  int j = start;
+  for (; j + U <= end; j += U) {
+    int c[U];
+    T x[U][V], a[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) c[u] = cols[j + u - off];
+#pragma unroll
+    for (int u = 0; u < U; ++u) ldv<T, V>(B1c + (int64_t)c[u] * ldb, x[u]);
+#pragma unroll
+    for (int u = 0; u < U; ++u) a[u] = vals[j + u - off];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int v = 0; v < V; ++v) acc[v] = fma(a[u], x[u][v], acc[v]);
+  }
+  for (; j < end; ++j) {
+    T x[V];
+    ldv<T, V>(B1c + (int64_t)cols[j - off] * ldb, x);
+    const T a = vals[j - off];
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] = fma(a, x[v], acc[v]);
+  }
+}
+
+template <typename T, int V, int G, int U, bool HQ, bool HS, bool HB>
+__global__ void __launch_bounds__(kThreads)
+direct_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
+              const T *__restrict__ val, int64_t n, int b, const T *__restrict__ Q, int64_t ldq,
+              const T *__restrict__ B1, const T *__restrict__ B2, int64_t ldb,
+              T *__restrict__ out, int64_t ldo, T ck, T alpha, T beta) {
+  constexpr int kRows = kThreads / G;
+  const int64_t row = (int64_t)blockIdx.x * kRows + threadIdx.x / G;
+  if (row >= n) return;
+  const int lane = threadIdx.x % G;
+  const int start = __ldg(rowptr + row);
+  const int end = __ldg(rowptr + row + 1);
+  for (int c0 = lane * V; c0 < b; c0 += G * V) {
+    T q[V], s[V], t[V], acc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] = T(0);
+    if constexpr (HQ) ldv<T, V>(Q + row * ldq + c0, q);
+    if constexpr (HS) ldv<T, V>(B1 + row * ldb + c0, s);
+    if constexpr (HB) ldv<T, V>(B2 + row * ldb + c0, t);
+    row_product<T, V, U>(colind, val, 0, start, end, B1 + c0, ldb, acc);
+    epilogue<T, V, HQ, HS, HB>(out + row * ldo + c0, acc, q, s, t, ck, alpha, beta);
+  }
+}
+
+template <typename T, int V, int G, int U, bool HQ, bool HS, bool HB>
+__global__ void __launch_bounds__(kThreads)
+staged_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
+              const T *__restrict__ val, int64_t n, int b, const T *__restrict__ Q, int64_t ldq,
+              const T *__restrict__ B1, const T *__restrict__ B2, int64_t ldb,
+              T *__restrict__ out, int64_t ldo, T ck, T alpha, T beta) {
+  constexpr int kRows = kThreads / G;
+  __shared__ int s_col[kStage];
+  __shared__ T s_val[kStage];
+  const int64_t row0 = (int64_t)blockIdx.x * kRows;
+  const int64_t rlast = min(n, row0 + kRows);
+  const int base = __ldg(rowptr + row0);
+  const int top = __ldg(rowptr + rlast);
+  const bool staged = top - base <= kStage;
+  if (staged) {
+    for (int i = threadIdx.x; i < top - base; i += kThreads) {
+      s_col[i] = __ldg(colind + base + i);
+      s_val[i] = __ldg(val + base + i);
+    }
+  }
+  __syncthreads();
+  const int64_t row = row0 + threadIdx.x / G;
+  if (row >= n) return;  // no barrier follows
+  const int lane = threadIdx.x % G;
+  const int start = __ldg(rowptr + row);
+  const int end = __ldg(rowptr + row + 1);
+  for (int c0 = lane * V; c0 < b; c0 += G * V) {
+    T q[V], s[V], t[V], acc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] = T(0);
+    if constexpr (HQ) ldv<T, V>(Q + row * ldq + c0, q);
+    if constexpr (HS) ldv<T, V>(B1 + row * ldb + c0, s);
+    if constexpr (HB) ldv<T, V>(B2 + row * ldb + c0, t);
+    if (staged) row_product<T, V, U>(s_col, s_val, base, start, end, B1 + c0, ldb, acc);
+    else row_product<T, V, U>(colind, val, 0, start, end, B1 + c0, ldb, acc);
+    epilogue<T, V, HQ, HS, HB>(out + row * ldo + c0, acc, q, s, t, ck, alpha, beta);
+  }
+}
+
+// ------------------------------------------------------------------ configurations
+// Encoded as fam | V << 4 | G << 8 | U << 16.
+inline int enc(int fam, int V, int G, int U) { return fam | (V << 4) | (G << 8) | (U << 16); }
+inline int fam_of(int c) { return c & 15; }
+inline int v_of(int c) { return (c >> 4) & 15; }
+inline int g_of(int c) { return (c >> 8) & 255; }
+inline int u_of(int c) { return c >> 16; }
+
+template <typename T>
+struct Args {
+  const sma_op *op;
+  cudaStream_t st;
+  int64_t b;
+  const T *Q;
+  int64_t ldq;
+  const T *B1, *B2;
+  int64_t ldb;
+  T *out;
+  int64_t ldo;
+  double ck, alpha, beta;
+};
+
+template <typename T, int V, int G, int U, bool HQ, bool HS, bool HB>
+void launch_one(int fam, const Args<T> &a) {
+  const T *val;
+  if constexpr (sizeof(T) == 8) val = (const T *)a.op->val64;
+  else val = (const T *)a.op->val32;
+  constexpr int kRows = kThreads / G;
+  const unsigned grid = (unsigned)((a.op->n + kRows - 1) / kRows);
+  if (fam == 0)
+    direct_kernel<T, V, G, U, HQ, HS, HB><<<grid, kThreads, 0, a.st>>>(
+        a.op->rowptr, a.op->colind, val, a.op->n, (int)a.b, a.Q, a.ldq, a.B1, a.B2, a.ldb, a.out,
+        a.ldo, (T)a.ck, (T)a.alpha, (T)a.beta);
+  else
+    staged_kernel<T, V, G, U, HQ, HS, HB><<<grid, kThreads, 0, a.st>>>(
+        a.op->rowptr, a.op->colind, val, a.op->n, (int)a.b, a.Q, a.ldq, a.B1, a.B2, a.ldb, a.out,
+        a.ldo, (T)a.ck, (T)a.alpha, (T)a.beta);
+  SMA_CHECK_LAUNCH();
+}
+
+template <typename T, int V, bool HQ, bool HS, bool HB>
+void launch_v(int c, const Args<T> &a) {
+  const int fam = fam_of(c);
+  switch (g_of(c) * 100 + u_of(c)) {
+    case 404: return launch_one<T, V, 4, 4, HQ, HS, HB>(fam, a);
+    case 408: return launch_one<T, V, 4, 8, HQ, HS, HB>(fam, a);
+    case 804: return launch_one<T, V, 8, 4, HQ, HS, HB>(fam, a);
+    case 808: return launch_one<T, V, 8, 8, HQ, HS, HB>(fam, a);
+    case 1604: return launch_one<T, V, 16, 4, HQ, HS, HB>(fam, a);
+    case 1608: return launch_one<T, V, 16, 8, HQ, HS, HB>(fam, a);
+    case 3204: return launch_one<T, V, 32, 4, HQ, HS, HB>(fam, a);
+    case 3208: return launch_one<T, V, 32, 8, HQ, HS, HB>(fam, a);
+    default: throw Error(SMA_ERR_INTERNAL, "bad CSR kernel configuration");
+  }
+}
+
+template <typename T, bool HQ, bool HS, bool HB>
+void launch_cfg(int c, const Args<T> &a) {
+  switch (v_of(c)) {
+    case 1: return launch_v<T, 1, HQ, HS, HB>(c, a);
+    case 2: return launch_v<T, 2, HQ, HS, HB>(c, a);
+    case 4: return launch_v<T, 4, HQ, HS, HB>(c, a);
+    default:
+      if constexpr (sizeof(T) == 4) {
+        if (v_of(c) == 8) return launch_v<T, 8, HQ, HS, HB>(c, a);
+      }
+      throw Error(SMA_ERR_INTERNAL, "bad CSR vector width");
+  }
+}
+
+inline bool aligned(const void *p, int bytes) { return p == nullptr || ((uintptr_t)p % bytes) == 0; }
+
+// Online autotuner.  The first 2 x (number of candidates) launches for a given operator,
+// element type, variant, width and leading dimension run the candidates in turn on the
+// real recurrence steps, bracketed by CUDA events; after the last of them one event
+// synchronization reads the times and the fastest candidate (best of its two runs) is
+// kept for the operator's lifetime.  Candidates: both families; the widest vector the
+// alignment allows, and half of it when that is 32 bytes; the narrowest power-of-two
+// group covering the block in one column pass, and the half-width group; U = 4 and 8.
+// Small operators (n < 20000) and contexts with autotuning off use the first candidate.
+template <typename T, bool HQ, bool HS, bool HB>
+void step(const Args<T> &a) {
+  const sma_op *op = a.op;
+  auto ok = [&](int v) {
+    const int bytes = std::min(16, v * (int)sizeof(T));
+    return a.b % v == 0 && a.ldb % v == 0 && a.ldo % v == 0 && (!HQ || a.ldq % v == 0) &&
+           aligned(a.Q, bytes) && aligned(a.B1, bytes) && aligned(a.B2, bytes) &&
+           aligned(a.out, bytes);
+  };
+  int vmax = 1;
+  for (int v : {2, 4, 8})
+    if (v * (int)sizeof(T) <= 32 && ok(v)) vmax = v;
+  const uint64_t key = ((uint64_t)sizeof(T) << 56) | ((uint64_t)vmax << 52) |
+                       ((uint64_t)((HQ ? 4 : 0) | (HS ? 2 : 0) | (HB ? 1 : 0)) << 48) |
+                       ((uint64_t)a.b << 24) | (uint64_t)std::min<int64_t>(a.ldb, 0xFFFFFF);
+  CsrTune &tu = const_cast<sma_op *>(op)->tuned[key];
+  if (tu.chosen >= 0) return launch_cfg<T, HQ, HS, HB>(tu.chosen, a);
+  if (tu.cands.empty()) {
+    for (int fam : {1, 0})
+      for (int V : {vmax, vmax / 2}) {
+        if (V < 1 || (V != vmax && vmax * (int)sizeof(T) < 32)) continue;
+        const int64_t lanes = (a.b + V - 1) / V;
+        const int g0 = lanes <= 4 ? 4 : lanes <= 8 ? 8 : lanes <= 16 ? 16 : 32;
+        for (int G : {g0, g0 / 2}) {
+          if (G < 4) continue;
+          tu.cands.push_back(enc(fam, V, G, 8));
+          tu.cands.push_back(enc(fam, V, G, 4));
+        }
+      }
+    if (!op->ctx->autotune || op->n < 20000) {
+      tu.chosen = tu.cands[0];
+      return launch_cfg<T, HQ, HS, HB>(tu.chosen, a);
+    }
+  }
+  constexpr int kReps = 2;
+  const size_t ncand = tu.cands.size();
+  const size_t idx = tu.trial.size();
+  const int c = tu.cands[idx % ncand];
+  cudaEvent_t e0, e1;
+  SMA_CUDA(cudaEventCreate(&e0));
+  SMA_CUDA(cudaEventCreate(&e1));
+  tu.events.push_back(e0);
+  tu.events.push_back(e1);
+  tu.trial.push_back(c);
+  SMA_CUDA(cudaEventRecord(e0, a.st));
+  launch_cfg<T, HQ, HS, HB>(c, a);
+  SMA_CUDA(cudaEventRecord(e1, a.st));
+  if (idx + 1 < kReps * ncand) return;
+  SMA_CUDA(cudaEventSynchronize(e1));
+  std::vector<float> best(ncand, INFINITY);
+  for (size_t i = 0; i < tu.trial.size(); ++i) {
+    float ms = 0.f;
+    SMA_CUDA(cudaEventElapsedTime(&ms, tu.events[2 * i], tu.events[2 * i + 1]));
+    best[i % ncand] = std::min(best[i % ncand], ms);
+  }
+  const size_t w = std::min_element(best.begin(), best.end()) - best.begin();
+  tu.chosen = tu.cands[w];
+  tu.release();
+  if (const char *vb = std::getenv("SMA_AUTOTUNE_VERBOSE"); vb && vb[0] == '1') {
+    fprintf(stderr, "sma autotune: %s n=%lld b=%lld ld=%lld variant=%d%d%d ->", sizeof(T) == 8 ? "fp64" : "fp32",
+            (long long)op->n, (long long)a.b, (long long)a.ldb, (int)HQ, (int)HS, (int)HB);
+    for (size_t i = 0; i < ncand; ++i)
+      fprintf(stderr, " %s%s/V%d/G%d/U%d=%.1fus", i == w ? "*" : "", fam_of(tu.cands[i]) ? "staged" : "direct",
+              v_of(tu.cands[i]), g_of(tu.cands[i]), u_of(tu.cands[i]), 1e3 * best[i]);
+    fprintf(stderr, "\n");
+  }
+}
+
+template <typename T>
+void clenshaw_step(const sma_op *op, cudaStream_t st, int64_t b, const T *Q, int64_t ldq,
+                   const T *B1, const T *B2, int64_t ldb, T *out, int64_t ldo, double ck,
+                   double alpha, double beta, bool has_self) {
+  const Args<T> a{op, st, b, Q, ldq, B1, B2, ldb, out, ldo, ck, alpha, beta};
+  if (Q && has_self && B2) return step<T, true, true, true>(a);
+  if (Q && has_self && !B2) return step<T, true, true, false>(a);
+  if (!Q && !has_self && !B2) return step<T, false, false, false>(a);
+  throw Error(SMA_ERR_INTERNAL, "unsupported Clenshaw step variant");
+}
+
+}  // namespace csr
+}  // namespace sma
+
+namespace sma {
+template <typename T>
+void csr_clenshaw_step(const sma_op *op, cudaStream_t st, int64_t b, const T *Q, int64_t ldq,
+                       const T *B1, const T *B2, int64_t ldb, T *out, int64_t ldo, double ck,
+                       double alpha, double beta, bool has_self) {
+  csr::clenshaw_step<T>(op, st, b, Q, ldq, B1, B2, ldb, out, ldo, ck, alpha, beta, has_self);
+}
+}  // namespace sma

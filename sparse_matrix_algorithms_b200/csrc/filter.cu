@@ -43,7 +43,7 @@ void op_apply(const sma_op *op, cudaStream_t st, const double *X, int64_t ldx, d
     require(ldx == ldy, SMA_ERR_ARG, "matrix-free operator callbacks need equal leading dimensions");
     const int rc = op->fn(op->user, X, Y, op->n, b, ldx, (void *)st);
     if (rc != 0) throw Error(SMA_ERR_CALLBACK, "matblock callback returned " + std::to_string(rc));
-    SMA_CHECK_LAUNCH();
+    SMA_CUDA(cudaGetLastError());
     return;
   }
   launch_clenshaw_step<double>(op, st, b, nullptr, 0, X, nullptr, ldx, Y, ldy, 0.0, 1.0, 0.0, false);

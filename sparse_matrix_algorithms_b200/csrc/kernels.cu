@@ -1,105 +1,27 @@
 // CUDA kernels of libsma (sm_100a).
 //
-// The hot one is the fused block Clenshaw step: one pass over the rows of a CSR
-// matrix that gathers the neighbour rows of B1, multiplies by the row's values and
-// finishes the three-term recurrence in the same pass,
+// The hot one, the fused block Clenshaw step
 //
 //     out[i,:] = ck*Q[i,:] + alpha*sum_j A[i,j]*B1[j,:] + beta*B1[i,:] - B2[i,:],
 //
-// replacing the reference's `mul!(AX,A,B1)` followed by a separate 4-array axpy sweep
-// (chebyshev_subspace_iteration.jl:573-582, polfed.jl:483-492).  AX never reaches
-// memory.  Blocks are row-major so that a row of B1 is one contiguous run of b
-// elements: a group of G threads owns one row and reads it with 16-byte vector loads
-// (V elements per thread), so every gather of a neighbour row is fully coalesced.
-// The kernel is HBM-bound (about 1 flop per byte); see clenshaw_step_bytes().
+// replaces the reference's `mul!(AX,A,B1)` followed by a separate 4-array axpy sweep
+// (chebyshev_subspace_iteration.jl:573-582, polfed.jl:483-492); AX never reaches memory.
+// Its CSR form lives in csr_clenshaw.cuh; this file holds the stencil form (the matrix-
+// free 1D Laplacian), the dispatcher, and the small kernels around the solvers.
 #include "sma_internal.h"
+#include "vec.cuh"
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 namespace sma {
+
+std::atomic<int64_t> g_kernel_launches{0};
+
 namespace {
 
 constexpr int kThreads = 256;
-
-// ------------------------------------------------------------------ vector fragments
-template <typename T, int V>
-struct Vec;
-template <> struct Vec<double, 1> { using type = double; };
-template <> struct Vec<double, 2> { using type = double2; };
-template <> struct Vec<float, 1> { using type = float; };
-template <> struct Vec<float, 2> { using type = float2; };
-template <> struct Vec<float, 4> { using type = float4; };
-
-template <typename T, int V>
-__device__ __forceinline__ void ldv(const T *__restrict__ p, T (&f)[V]) {
-  using VT = typename Vec<T, V>::type;
-  const VT x = __ldg(reinterpret_cast<const VT *>(p));
-  if constexpr (V == 1) {
-    f[0] = x;
-  } else if constexpr (V == 2) {
-    f[0] = x.x; f[1] = x.y;
-  } else {
-    f[0] = x.x; f[1] = x.y; f[2] = x.z; f[3] = x.w;
-  }
-}
-
-template <typename T, int V>
-__device__ __forceinline__ void stv(T *__restrict__ p, const T (&f)[V]) {
-  using VT = typename Vec<T, V>::type;
-  VT x;
-  if constexpr (V == 1) {
-    x = f[0];
-  } else if constexpr (V == 2) {
-    x.x = f[0]; x.y = f[1];
-  } else {
-    x.x = f[0]; x.y = f[1]; x.z = f[2]; x.w = f[3];
-  }
-  *reinterpret_cast<VT *>(p) = x;
-}
-
-// ------------------------------------------------------------------ operator rows
-// CSR rows: acc += sum_j val[j] * B1[colind[j], c0:c0+V], terms in ascending j.
-template <typename T>
-struct CsrRows {
-  const int *__restrict__ rowptr;
-  const int *__restrict__ colind;
-  const T *__restrict__ val;
-
-  template <int V>
-  __device__ __forceinline__ void product(int64_t row, const T *__restrict__ B1, int64_t ldb,
-                                          int c0, T (&acc)[V]) const {
-    int j = __ldg(rowptr + row);
-    const int e = __ldg(rowptr + row + 1);
-    // Unrolled by 4 so that four independent neighbour-row gathers are in flight.
-    for (; j + 3 < e; j += 4) {
-      const int k0 = __ldg(colind + j), k1 = __ldg(colind + j + 1);
-      const int k2 = __ldg(colind + j + 2), k3 = __ldg(colind + j + 3);
-      const T a0 = __ldg(val + j), a1 = __ldg(val + j + 1);
-      const T a2 = __ldg(val + j + 2), a3 = __ldg(val + j + 3);
-      T x0[V], x1[V], x2[V], x3[V];
-      ldv<T, V>(B1 + (int64_t)k0 * ldb + c0, x0);
-      ldv<T, V>(B1 + (int64_t)k1 * ldb + c0, x1);
-      ldv<T, V>(B1 + (int64_t)k2 * ldb + c0, x2);
-      ldv<T, V>(B1 + (int64_t)k3 * ldb + c0, x3);
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        acc[v] = fma(a0, x0[v], acc[v]);
-        acc[v] = fma(a1, x1[v], acc[v]);
-        acc[v] = fma(a2, x2[v], acc[v]);
-        acc[v] = fma(a3, x3[v], acc[v]);
-      }
-    }
-    for (; j < e; ++j) {
-      const int k0 = __ldg(colind + j);
-      const T a0 = __ldg(val + j);
-      T x0[V];
-      ldv<T, V>(B1 + (int64_t)k0 * ldb + c0, x0);
-#pragma unroll
-      for (int v = 0; v < V; ++v) acc[v] = fma(a0, x0[v], acc[v]);
-    }
-  }
-};
 
 // tridiag(-1,2,-1) stencil, evaluated as the reference's lap1d_matblock!
 // (polfed.jl:1209-1219): Y[1]=2X[1]-X[2]; Y[i]=-X[i-1]+2X[i]-X[i+1]; Y[n]=-X[n-1]+2X[n].
@@ -128,10 +50,10 @@ struct Lap1dRows {
   }
 };
 
-// ------------------------------------------------------------------ fused Clenshaw step
+// ------------------------------------------------------------------ stencil Clenshaw step
 template <typename T, int V, int G, bool HAS_Q, bool HAS_SELF, bool HAS_B2, typename Rows>
 __global__ void __launch_bounds__(kThreads)
-clenshaw_step_kernel(Rows rows, int64_t n, int b, const T *__restrict__ Q, int64_t ldq,
+stencil_step_kernel(Rows rows, int64_t n, int b, const T *__restrict__ Q, int64_t ldq,
                      const T *__restrict__ B1, const T *__restrict__ B2, int64_t ldb,
                      T *__restrict__ out, int64_t ldo, T ck, T alpha, T beta) {
   constexpr int kRows = kThreads / G;
@@ -167,7 +89,7 @@ void launch_cfg(const Rows &rows, cudaStream_t st, int64_t n, int64_t b, const T
   constexpr int kRows = kThreads / G;
   const int64_t need = (n + kRows - 1) / kRows;
   const int grid = (int)std::min<int64_t>(need, 148LL * 256);
-  clenshaw_step_kernel<T, V, G, HQ, HS, HB, Rows><<<grid, kThreads, 0, st>>>(
+  stencil_step_kernel<T, V, G, HQ, HS, HB, Rows><<<grid, kThreads, 0, st>>>(
       rows, n, (int)b, Q, ldq, B1, B2, ldb, out, ldo, (T)ck, (T)alpha, (T)beta);
 }
 
@@ -486,19 +408,14 @@ void launch_clenshaw_step(const sma_op *op, cudaStream_t st, int64_t b, const T 
                           double alpha, double beta, bool has_self) {
   if (op->n == 0 || b == 0) return;
   if (op->kind == OP_CSR) {
-    CsrRows<T> rows;
-    rows.rowptr = op->rowptr;
-    rows.colind = op->colind;
-    if constexpr (sizeof(T) == 8) rows.val = (const T *)op->val64;
-    else rows.val = (const T *)op->val32;
-    dispatch_flags<T>(rows, st, op->n, b, Q, ldq, B1, B2, ldb, out, ldo, ck, alpha, beta, has_self);
+    csr_clenshaw_step<T>(op, st, b, Q, ldq, B1, B2, ldb, out, ldo, ck, alpha, beta, has_self);
   } else if (op->kind == OP_LAP1D) {
     Lap1dRows<T> rows{op->n};
     dispatch_flags<T>(rows, st, op->n, b, Q, ldq, B1, B2, ldb, out, ldo, ck, alpha, beta, has_self);
+    SMA_CHECK_LAUNCH();
   } else {
     throw Error(SMA_ERR_INTERNAL, "fused Clenshaw step needs a device operator");
   }
-  SMA_CHECK_LAUNCH();
 }
 
 template <typename T>

@@ -5,8 +5,10 @@
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -49,11 +51,36 @@ void set_last_error(const std::string &msg);
                                            std::to_string((int)s_));                    \
   } while (0)
 
-#define SMA_CHECK_LAUNCH() SMA_CUDA(cudaGetLastError())
+// Every launch of this library's own kernels goes through SMA_CHECK_LAUNCH, which
+// also counts it (sma_stats.kernel_launches).
+extern std::atomic<int64_t> g_kernel_launches;
+#define SMA_CHECK_LAUNCH()                                                     \
+  do {                                                                         \
+    ::sma::g_kernel_launches.fetch_add(1, std::memory_order_relaxed);          \
+    SMA_CUDA(cudaGetLastError());                                              \
+  } while (0)
 
 inline void require(bool ok, int code, const std::string &msg) {
   if (!ok) throw Error(code, msg);
 }
+
+// Online autotuner state of the CSR Clenshaw step for one (element type, vector width,
+// variant, block width, leading dimension) key of an operator (csr_clenshaw.cuh).
+struct CsrTune {
+  std::vector<int> cands;           // encoded candidate configurations
+  std::vector<int> trial;           // configuration of each timed launch so far
+  std::vector<cudaEvent_t> events;  // start/stop event pair per timed launch
+  int chosen = -1;                  // encoded winner once decided
+  CsrTune() = default;
+  CsrTune(const CsrTune &) = delete;
+  CsrTune &operator=(const CsrTune &) = delete;
+  void release() {
+    for (cudaEvent_t e : events) cudaEventDestroy(e);
+    events.clear();
+    trial.clear();
+  }
+  ~CsrTune() { release(); }
+};
 
 }  // namespace sma
 
@@ -64,6 +91,7 @@ struct sma_ctx {
   cublasHandle_t cublas = nullptr;
   cusolverDnHandle_t cusolver = nullptr;
   int num_sms = 148;
+  bool autotune = true;  // SMA_AUTOTUNE=0 in the environment turns the kernel autotuner off
 };
 
 enum op_kind { OP_CSR = 0, OP_LAP1D = 1, OP_MATBLOCK = 2 };
@@ -84,6 +112,8 @@ struct sma_op {
   // caller callback
   sma_matblock_fn fn = nullptr;
   void *user = nullptr;
+  // autotuned CSR kernel configurations
+  std::map<uint64_t, sma::CsrTune> tuned;
 };
 
 namespace sma {
@@ -133,6 +163,11 @@ template <typename T>
 void launch_clenshaw_step(const sma_op *op, cudaStream_t st, int64_t b, const T *Q, int64_t ldq,
                           const T *B1, const T *B2, int64_t ldb, T *out, int64_t ldo, double ck,
                           double alpha, double beta, bool has_self);
+// The CSR form of launch_clenshaw_step (csr_clenshaw_f64.cu / csr_clenshaw_f32.cu).
+template <typename T>
+void csr_clenshaw_step(const sma_op *op, cudaStream_t st, int64_t b, const T *Q, int64_t ldq,
+                       const T *B1, const T *B2, int64_t ldb, T *out, int64_t ldo, double ck,
+                       double alpha, double beta, bool has_self);
 // out = ck * Q
 template <typename T>
 void launch_scale_block(cudaStream_t st, int64_t n, int64_t b, const T *Q, int64_t ldq, T *out,

@@ -162,6 +162,7 @@ sma_result *empty_result(sma_ctx *ctx, int64_t n) {
 // overload, matrix_free = 0) and 771-848 (matrix-free overload, matrix_free = 1).
 sma_result *cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts &o) {
   const auto t0 = std::chrono::steady_clock::now();
+  const int64_t launches0 = g_kernel_launches.load();
   sma_ctx *ctx = op->ctx;
   cudaStream_t st = ctx->stream;
   const bool mf = o.matrix_free != 0;
@@ -304,6 +305,7 @@ sma_result *cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts
     r = make_result(ctx, n, X.p, m0, idx, take(lam, idx), take(res, idx));
   }
   stats.total_ms = ms_since(t0);
+  stats.kernel_launches = g_kernel_launches.load() - launches0;
   r->stats = stats;
   return r;
 }
@@ -336,6 +338,7 @@ RitzSet rayleigh(const sma_op *op, cudaStream_t st, int64_t n, int64_t k, const 
 // build_full_basis! (polfed.jl:1022-1099) and extract_pairs (polfed.jl:892-984).
 sma_result *polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polfed_opts &o) {
   const auto t0 = std::chrono::steady_clock::now();
+  const int64_t launches0 = g_kernel_launches.load();
   sma_ctx *ctx = op->ctx;
   cudaStream_t st = ctx->stream;
   const int64_t n = op->n;
@@ -459,6 +462,7 @@ sma_result *polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polf
     stats.orth_ms = ph[PH_ORTH];
     stats.rr_ms = ph[PH_RR];
     stats.total_ms = ms_since(t0);
+    stats.kernel_launches = g_kernel_launches.load() - launches0;
     r->stats = stats;
     return r;
   };

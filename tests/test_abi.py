@@ -41,13 +41,34 @@ def test_python_bindings_cover_the_header(lib_built):
     L.load()
 
 
+def _header_struct_members(name):
+    """Member names (reserved arrays expanded) of `typedef struct name {...}` in sma.h."""
+    src = open(os.path.join(ROOT, "include", "sma.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), src, flags=re.S).group(1)
+    members = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        typ, rest = decl.split(None, 1)
+        assert typ in ("int64_t", "double"), decl
+        for m in rest.split(","):
+            m = m.strip()
+            arr = re.match(r"(\w+)\[(\d+)\]", m)
+            members += [arr.group(1)] * int(arr.group(2)) if arr else [m]
+    return members
+
+
 def test_struct_layouts_match_header(lib_built):
     from sparse_matrix_algorithms_b200 import _lib as L
 
-    # every field is 8 bytes wide and the structs end with 8 reserved slots
-    assert ctypes.sizeof(L.ChebOpts) == 8 * (len(L.ChebOpts._fields_) - 1 + 8)
-    assert ctypes.sizeof(L.PolfedOpts) == 8 * (len(L.PolfedOpts._fields_) - 1 + 8)
-    assert ctypes.sizeof(L.Stats) == 8 * (len(L.Stats._fields_) - 1 + 8)
+    for cname, pyst in [("sma_cheb_opts", L.ChebOpts), ("sma_polfed_opts", L.PolfedOpts),
+                        ("sma_stats", L.Stats)]:
+        members = _header_struct_members(cname)
+        assert ctypes.sizeof(pyst) == 8 * len(members), cname
+        named = [m for m in dict.fromkeys(members) if m != "reserved"]
+        assert [f for f, _ in pyst._fields_ if f != "reserved"] == named, cname
     o = L.ChebOpts()
     L.load().sma_cheb_opts_default(ctypes.byref(o))
     assert (o.m0, o.degree, o.maxiter, o.tol, o.res_gate, o.seed) == (200, 80, 8, 1e-10, 1e-6, 1)

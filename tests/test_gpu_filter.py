@@ -1,0 +1,170 @@
+"""GPU parity of the hot path: the block Clenshaw filter (apply_poly_block!) and the
+sparse block product, through the C ABI, against the CPU oracle on identical inputs.
+
+Tolerances: FP64 results agree with the oracle to 1e-12 relative to the block's
+magnitude (the GPU fuses multiply-adds, the oracle rounds twice, and the recurrence
+runs K steps).  The FP32 filter is compared with the FP64 oracle at 2e-4 relative.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import sma_oracle as O
+from sparse_matrix_algorithms_b200 import matrices as M
+
+pytestmark = pytest.mark.gpu
+
+
+def _ragged(n, seed):
+    """Symmetric matrix with empty, short and long rows (ragged CSR)."""
+    rng = np.random.default_rng(seed)
+    rows, cols = [], []
+    for i in range(n):
+        k = [0, 1, 2, 5, 13][i % 5]
+        js = rng.integers(0, n, size=k)
+        rows += [i] * k
+        cols += list(js)
+    A = sp.coo_matrix((rng.uniform(-1, 1, len(rows)), (rows, cols)), shape=(n, n)).tocsr()
+    A = A + A.T
+    A.setdiag(np.where(np.arange(n) % 7 == 3, 0.0, rng.uniform(-2, 2, n)))
+    A.eliminate_zeros()
+    return M._canonical(A)
+
+
+MATRICES = {
+    "lap1d": lambda: M.lap1d(700),
+    "anderson_L8": lambda: M.anderson3d(8, 16.5, 2),
+    "xxz_L12": lambda: M.xxz_sz0(12, 5.0, 1),
+    "ragged": lambda: _ragged(333, 4),
+}
+
+
+def _bounds(A):
+    return O.gershgorin_bounds(A)
+
+
+@pytest.mark.parametrize("name", sorted(MATRICES))
+@pytest.mark.parametrize("b", [1, 2, 3, 8, 17, 32, 64, 100])
+def test_filter_fp64_matches_oracle(lib_built, name, b):
+    import sparse_matrix_algorithms_b200 as S
+
+    A = MATRICES[name]()
+    smin, smax = _bounds(A)
+    Q = M.splitmix_normal(b, A.shape[0], b)
+    for K, window in [(0, "step"), (1, "delta"), (2, "step"), (37, "smooth"), (160, "step")]:
+        c = O.build_coeffs(K, smin, smax, 0.1, -0.4, 0.3, window, True)
+        ref = O.apply_poly_block(A, Q, c, smin, smax)
+        got = S.apply_poly_block(A, Q, c, smin, smax)
+        scale = max(np.abs(ref).max(), np.abs(Q).max())
+        assert np.abs(got - ref).max() <= 1e-12 * scale, (K, window)
+
+
+@pytest.mark.parametrize("b", [1, 4, 6, 32, 96])
+def test_filter_fp32_close_to_oracle(lib_built, b):
+    import sparse_matrix_algorithms_b200 as S
+
+    A = M.anderson3d(8, 16.5, 2)
+    smin, smax = _bounds(A)
+    Q = M.splitmix_normal(7, A.shape[0], b)
+    c = O.build_coeffs(120, smin, smax, 0.0, -0.5, 0.5, "step", True)
+    ref = O.apply_poly_block(A, Q, c, smin, smax)
+    got = S.apply_poly_block(A, Q, c, smin, smax, precision="fp32")
+    assert np.abs(got - ref).max() <= 2e-4 * np.abs(ref).max()
+
+
+def test_identity_filter_returns_q(lib_built):
+    import sparse_matrix_algorithms_b200 as S
+
+    A = M.xxz_sz0(10, 3.0, 5)
+    Q = M.splitmix_normal(1, A.shape[0], 16)
+    c = O.cheb_window_coeffs(-1.0, 1.0, 80, jackson=True)
+    Y = S.apply_poly_block(A, Q, c, *_bounds(A))
+    assert np.abs(Y - Q).max() < 1e-12 * np.abs(Q).max()
+
+
+def test_lap1d_stencil_operator_matches_csr_oracle(lib_built):
+    import sparse_matrix_algorithms_b200 as S
+
+    n = 1234
+    op = S.Lap1dOperator(n)
+    Q = M.splitmix_normal(9, n, 24)
+    for K in [0, 1, 5, 200]:
+        c = O.build_coeffs(K, 0.0, 4.0, 2.0, 1.9, 2.2, "delta", True)
+        ref = O.apply_poly_block(M.lap1d(n), Q, c, 0.0, 4.0)
+        got = S.apply_poly_block(op, Q, c, 0.0, 4.0)
+        assert np.abs(got - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
+
+
+def _device(arr):
+    import torch
+
+    return torch.as_tensor(np.ascontiguousarray(arr), device="cuda")
+
+
+def test_device_entry_with_padded_leading_dimension(lib_built):
+    """sma_apply_poly_block_dev on row-major device blocks with ld > b."""
+    import torch
+    import sparse_matrix_algorithms_b200 as S
+    from sparse_matrix_algorithms_b200 import _lib as L
+
+    A = M.anderson3d(7, 16.5, 1)
+    n, b, ldq, ldy = A.shape[0], 10, 13, 16
+    smin, smax = _bounds(A)
+    op = S.SparseOperator(A)
+    Q = M.splitmix_normal(4, n, b)
+    Qpad = np.zeros((n, ldq))
+    Qpad[:, :b] = Q
+    dQ = _device(Qpad)
+    dY = torch.full((n, ldy), 7.0, dtype=torch.float64, device="cuda")
+    c = np.ascontiguousarray(O.build_coeffs(45, smin, smax, 0.0, -1.0, 1.5, "step", True))
+    torch.cuda.synchronize()
+    L.check(L.load().sma_apply_poly_block_dev(op.handle, c.ctypes.data, len(c) - 1, smin, smax,
+                                              dQ.data_ptr(), ldq, dY.data_ptr(), ldy, b, 0))
+    Y = dY.cpu().numpy()
+    ref = O.apply_poly_block(A, Q, c, smin, smax)
+    assert np.abs(Y[:, :b] - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert np.all(Y[:, b:] == 7.0)  # padding untouched
+
+
+def test_spmm_dev_matches_scipy(lib_built):
+    import torch
+    import sparse_matrix_algorithms_b200 as S
+    from sparse_matrix_algorithms_b200 import _lib as L
+
+    A = _ragged(500, 9)
+    op = S.SparseOperator(A)
+    X = M.splitmix_normal(2, 500, 33)
+    dX = _device(X)
+    dY = torch.empty((500, 33), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    L.check(L.load().sma_spmm_dev(op.handle, dX.data_ptr(), 33, dY.data_ptr(), 33, 33))
+    assert np.abs(dY.cpu().numpy() - A @ X).max() < 1e-13 * np.abs(A @ X).max()
+
+
+def test_empty_block_and_empty_matrix(lib_built):
+    import sparse_matrix_algorithms_b200 as S
+
+    A = M.lap1d(50)
+    Y = S.apply_poly_block(A, np.zeros((50, 0)), [1.0, 0.5], 0.0, 4.0)
+    assert Y.shape == (50, 0)
+    E = sp.csr_matrix((0, 0))
+    Y = S.apply_poly_block(E, np.zeros((0, 3)), [1.0, 0.5], 0.0, 4.0)
+    assert Y.shape == (0, 3)
+
+
+def test_invalid_csr_is_rejected_before_upload(lib_built):
+    import sparse_matrix_algorithms_b200 as S
+    from sparse_matrix_algorithms_b200 import _lib as L
+
+    ctx = S.context()
+    colptr = np.array([0, 2, 3], dtype=np.int64)
+    rowval = np.array([1, 0, 5], dtype=np.int64)  # unsorted and out of range
+    nzval = np.ones(3)
+    h = ctypes.c_void_p()
+    rc = L.load().sma_op_create_csc(ctx.handle, 2, 3, colptr.ctypes.data, rowval.ctypes.data,
+                                    nzval.ctypes.data, 0, 0, ctypes.byref(h))
+    assert rc == L.SMA_ERR_ARG
+    with pytest.raises(S.ArgumentError):
+        S.SparseOperator(sp.csr_matrix(np.array([[1.0, 2.0], [0.0, 1.0]])), check_symmetric=True)

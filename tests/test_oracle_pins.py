@@ -133,12 +133,18 @@ def test_published_runs_fixture_is_consistent():
 
 @pytest.mark.slow
 def test_oracle_reproduces_published_polfed_n10000():
-    """polfed.jl:1279-1288: n=10000, nev=1000, s=64, degree=32, b=5 (mmax=79), :smooth
-    -> inside=1000, maxres 3.1e-14.  The oracle's run is stored in
-    tests/golden/oracle_published_polfed_n10000.json by make_golden.py."""
+    """polfed.jl:1279-1288: n=10000, nev=1000, s=64, degree=32, b=5 (mmax=79)
+    -> inside=1000, maxres 3.1e-14.  The harness window ends sit exactly on eigenvalues
+    (polfed.jl:1223-1233), so the two boundary pairs fall inside or outside by rounding;
+    the reference's own runs report 998-1000.  The oracle's runs (make_golden.py) are
+    stored in tests/golden/oracle_published_polfed_n10000.json."""
     path = os.path.join(GOLDEN, "oracle_published_polfed_n10000.json")
     with open(path) as f:
         g = json.load(f)
-    assert g["inside"] == 1000
-    assert g["maxres"] < 1e-12
-    assert g["max_abs_err_vs_exact"] < 1e-12
+    pub = json.load(open(os.path.join(GOLDEN, "published_runs.json")))["runs"][1]
+    assert pub["n"] == 10000 and pub["found"] == 1000
+    for run in g["runs"].values():
+        assert 998 <= run["inside"] <= 1000
+        assert run["matched"] >= 998 and run["spurious"] == 0
+        assert run["maxres"] < 10 * pub["maxres"]
+        assert run["max_abs_err_vs_exact"] < 1e-12
