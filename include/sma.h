@@ -187,6 +187,18 @@ int sma_apply_poly_block(sma_op *op, const double *coeffs, int64_t K, double smi
 /* Y = A X on device row-major FP64 blocks (apply_A_block!). Synchronous. */
 int sma_spmm_dev(sma_op *op, const double *X_dev, int64_t ldx, double *Y_dev, int64_t ldy,
                  int64_t b);
+/* The FP64 filter of sma_apply_poly_block_dev without any device allocation, for callers
+ * that cannot allocate device memory: processes whose GPU memory another allocator has
+ * reserved up front, or latency-critical loops that must not pay for cudaMalloc/cudaFree.
+ * No counterpart in the reference (its filter allocates Julia arrays).  Its three n x b
+ * recurrence blocks live in one static device array of 48 MiB (held on every device that
+ * loads it until exit), so n*b must be <= 2,097,152 (else SMA_ERR_ARG).  Device operators
+ * only (CSR or stencil).  All calls on a device share the array: calls that overlap on
+ * the GPU race, so serialize them.  The first call on a device looks the array up; make
+ * it before any stream capture.  Synchronous. */
+int sma_apply_poly_block_noalloc(sma_op *op, const double *coeffs, int64_t K, double smin,
+                                 double smax, const double *Q_dev, int64_t ldq, double *Y_dev,
+                                 int64_t ldy, int64_t b);
 
 /* ---------------------------------------------------------------- solvers */
 void sma_cheb_opts_default(sma_cheb_opts *o);

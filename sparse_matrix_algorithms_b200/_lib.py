@@ -115,6 +115,8 @@ SIGNATURES = [
     ("sma_apply_poly_block", c_int, [c_void_p, c_void_p, c_int64, c_double, c_double, c_void_p,
                                      c_void_p, c_int64, c_int64]),
     ("sma_spmm_dev", c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_int64]),
+    ("sma_apply_poly_block_noalloc", c_int, [c_void_p, c_void_p, c_int64, c_double, c_double,
+                                             c_void_p, c_int64, c_void_p, c_int64, c_int64]),
     ("sma_cheb_opts_default", None, [ctypes.POINTER(ChebOpts)]),
     ("sma_polfed_opts_default", None, [ctypes.POINTER(PolfedOpts)]),
     ("sma_cheb_solve", c_int, [c_void_p, c_double, c_double, ctypes.POINTER(ChebOpts),

@@ -309,3 +309,44 @@ void csr_clenshaw_step(const sma_op *op, cudaStream_t st, int64_t b, const T *Q,
   csr::clenshaw_step<T>(op, st, b, Q, ldq, B1, B2, ldb, out, ldo, ck, alpha, beta, has_self);
 }
 }  // namespace sma
+
+namespace sma {
+namespace csr {
+
+// The CSR step without the autotuner: the operator's tuned configuration for this key when
+// one has been chosen, else the autotuner's first candidate.  Creates no events and never
+// inserts into the tuning cache (used by the allocation-free entry point).
+template <typename T, bool HQ, bool HS, bool HB>
+void step_untuned(const Args<T> &a) {
+  auto ok = [&](int v) {
+    const int bytes = std::min(16, v * (int)sizeof(T));
+    return a.b % v == 0 && a.ldb % v == 0 && a.ldo % v == 0 && (!HQ || a.ldq % v == 0) &&
+           aligned(a.Q, bytes) && aligned(a.B1, bytes) && aligned(a.B2, bytes) &&
+           aligned(a.out, bytes);
+  };
+  int vmax = 1;
+  for (int v : {2, 4, 8})
+    if (v * (int)sizeof(T) <= 32 && ok(v)) vmax = v;
+  const uint64_t key = ((uint64_t)sizeof(T) << 56) | ((uint64_t)vmax << 52) |
+                       ((uint64_t)((HQ ? 4 : 0) | (HS ? 2 : 0) | (HB ? 1 : 0)) << 48) |
+                       ((uint64_t)a.b << 24) | (uint64_t)std::min<int64_t>(a.ldb, 0xFFFFFF);
+  const auto it = a.op->tuned.find(key);
+  if (it != a.op->tuned.end() && it->second.chosen >= 0)
+    return launch_cfg<T, HQ, HS, HB>(it->second.chosen, a);
+  const int64_t lanes = (a.b + vmax - 1) / vmax;
+  const int g0 = lanes <= 4 ? 4 : lanes <= 8 ? 8 : lanes <= 16 ? 16 : 32;
+  launch_cfg<T, HQ, HS, HB>(enc(1, vmax, g0, 8), a);
+}
+
+}  // namespace csr
+
+template <typename T>
+void csr_clenshaw_step_untuned(const sma_op *op, cudaStream_t st, int64_t b, const T *Q,
+                               int64_t ldq, const T *B1, const T *B2, int64_t ldb, T *out,
+                               int64_t ldo, double ck, double alpha, double beta, bool has_self) {
+  const csr::Args<T> a{op, st, b, Q, ldq, B1, B2, ldb, out, ldo, ck, alpha, beta};
+  if (Q && has_self && B2) return csr::step_untuned<T, true, true, true>(a);
+  if (Q && has_self && !B2) return csr::step_untuned<T, true, true, false>(a);
+  throw Error(SMA_ERR_INTERNAL, "unsupported Clenshaw step variant");
+}
+}  // namespace sma
