@@ -50,8 +50,10 @@ enum sma_status {
 
 enum sma_window { SMA_WINDOW_STEP = 0, SMA_WINDOW_DELTA = 1, SMA_WINDOW_SMOOTH = 2 };
 
-/* Arithmetic of the block Clenshaw filter.  FP64 is the reference's arithmetic. */
-enum sma_precision { SMA_PREC_FP64 = 0, SMA_PREC_FP32 = 1 };
+/* Arithmetic of the block Clenshaw filter.  FP64 is the reference's arithmetic.  MIXED
+ * (solvers only) filters in FP32 while that still reduces the residuals, then in FP64 for
+ * the final iterations; orthogonalization, Rayleigh-Ritz and residuals are always FP64. */
+enum sma_precision { SMA_PREC_FP64 = 0, SMA_PREC_FP32 = 1, SMA_PREC_MIXED = 2 };
 
 typedef struct sma_ctx sma_ctx;
 typedef struct sma_op sma_op;
@@ -83,7 +85,12 @@ typedef struct sma_cheb_opts {
                              chebyshev_subspace_iteration.jl:731-749); 1: matrix-free overload
                              semantics (two_hit early exit, chebyshev_subspace_iteration.jl:827-836) */
   int64_t precision;      /* enum sma_precision of the filter, default SMA_PREC_FP64 */
-  int64_t reserved[8];
+  int64_t lock;           /* 1: lock converged pairs (an extension: the reference's TODO at
+                             chebyshev_subspace_iteration.jl:117 and its unused append_locked!,
+                             :282-290).  Pairs inside [emin, emax] with residual < tol leave
+                             the filtered block; later blocks are orthogonalized against them.
+                             Default 0 (the reference's behaviour). */
+  int64_t reserved[7];
 } sma_cheb_opts;
 
 /* Keyword arguments of polfed (polfed.jl:1128). */
@@ -125,7 +132,10 @@ typedef struct sma_stats {
   int64_t warnings;       /* bit 0: interval outside the spectral bounds */
   int64_t kernel_launches; /* this library's own CUDA kernels launched by the solve
                               (cuBLAS / cuSOLVER launches not included) */
-  int64_t reserved[7];
+  int64_t fp32_filter_calls; /* filter applications run in FP32 (FP32 / MIXED precision) */
+  int64_t locked;         /* pairs locked during the solve (Chebyshev with lock = 1) */
+  int64_t polish_iterations; /* FP64 polishing iterations after an FP32 POLFED basis */
+  int64_t reserved[4];
 } sma_stats;
 
 /* ---------------------------------------------------------------- library, context */
@@ -149,6 +159,17 @@ int sma_op_create_csc(sma_ctx *ctx, int64_t n, int64_t nnz, const int64_t *colpt
 /* Matrix-free 1D Laplacian tridiag(-1,2,-1) as a device stencil (the reference's
  * lap1d_matblock!, polfed.jl:1209-1219). */
 int sma_op_create_lap1d(sma_ctx *ctx, int64_t n, sma_op **out);
+/* Matrix-free 3D Anderson model on an L^3 periodic lattice (L >= 3) as a device stencil:
+ * eps[i] (i = x + L*(y + L*z), L^3 host doubles) on the diagonal, hopping t to the six
+ * neighbours.  Products are bit-identical to the stored CSR matrix's.  An extension that
+ * gives the reference's matrix-free signatures (MatrixFreeRealSymOp, polfed.jl:165) a GPU
+ * operator for this model with no index arrays. */
+int sma_op_create_anderson(sma_ctx *ctx, int64_t L, const double *eps, double t, sma_op **out);
+/* Matrix-free random-field XXZ chain (even L in 4..30, periodic) in the Sz = 0 sector as a
+ * device stencil: H = J sum (SxSx + SySy + Delta SzSz) + sum h_i Sz_i, S = sigma/2, basis
+ * ordered by the states' integer values (bit i = site i up); h holds L host doubles. */
+int sma_op_create_xxz(sma_ctx *ctx, int64_t L, double J, double Delta, const double *h,
+                      sma_op **out);
 /* Matrix-free operator from a caller-supplied device block callback
  * (MatrixFreeRealSymOp(n, matvec!, matblock!), polfed.jl:165). */
 int sma_op_create_matblock(sma_ctx *ctx, int64_t n, sma_matblock_fn fn, void *user,
@@ -157,6 +178,12 @@ int sma_op_destroy(sma_op *op);
 int sma_op_info(const sma_op *op, int64_t *n, int64_t *nnz);
 /* Gershgorin bounds (chebyshev_subspace_iteration.jl:351-367); explicit matrices only. */
 int sma_gershgorin_bounds(sma_op *op, double *smin, double *smax);
+/* Tighter spectral bounds than Gershgorin's (an extension; the reference has only
+ * gershgorin_bounds): `steps` Lanczos steps in FP64 with full reorthogonalization from a
+ * seeded random vector; the extreme Ritz values widened by their residual norms (at least
+ * 1e-3 of the Ritz range), clipped to the Gershgorin interval when the operator has one
+ * (explicit matrices, model stencils).  An estimate.  Any operator kind. */
+int sma_lanczos_bounds(sma_op *op, int64_t steps, int64_t seed, double *smin, double *smax);
 
 /* ---------------------------------------------------------------- filter coefficients */
 /* jackson_kernel(K): g[0..K] (chebyshev_subspace_iteration.jl:376-387). */

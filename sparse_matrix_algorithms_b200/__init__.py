@@ -7,7 +7,9 @@ package is its Python mirror of the reference's API plus the seeded test-matrix
 generators.
 """
 from .api import (  # noqa: F401
+    AndersonOperator,
     ArgumentError,
+    XXZOperator,
     Context,
     DeviceMatblock,
     Lap1dOperator,
@@ -23,6 +25,7 @@ from .api import (  # noqa: F401
     context,
     gershgorin_bounds,
     jackson_kernel,
+    lanczos_bounds,
     polfed,
 )
 from . import matrices  # noqa: F401

@@ -33,7 +33,7 @@ SMA_ERR_CALLBACK = 10
 SMA_ERR_INTERNAL = 11
 
 WINDOWS = {"step": 0, "delta": 1, "smooth": 2}
-PRECISIONS = {"fp64": 0, "fp32": 1}
+PRECISIONS = {"fp64": 0, "fp32": 1, "mixed": 2}
 
 
 class SMAError(RuntimeError):
@@ -59,7 +59,7 @@ class ChebOpts(ctypes.Structure):
                 ("maxiter", c_int64), ("tol", c_double), ("res_gate", c_double),
                 ("jackson", c_int64), ("debug", c_int64), ("two_hit", c_int64),
                 ("seed", c_int64), ("window_type", c_int64), ("matrix_free", c_int64),
-                ("precision", c_int64), ("reserved", c_int64 * 8)]
+                ("precision", c_int64), ("lock", c_int64), ("reserved", c_int64 * 7)]
 
 
 class PolfedOpts(ctypes.Structure):
@@ -78,7 +78,8 @@ class Stats(ctypes.Structure):
                 ("spmm_columns", c_int64), ("filter_ms", c_double), ("orth_ms", c_double),
                 ("rr_ms", c_double), ("total_ms", c_double), ("filter_bytes", c_double),
                 ("qr_fallbacks", c_int64), ("warnings", c_int64), ("kernel_launches", c_int64),
-                ("reserved", c_int64 * 7)]
+                ("fp32_filter_calls", c_int64), ("locked", c_int64),
+                ("polish_iterations", c_int64), ("reserved", c_int64 * 4)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
@@ -98,11 +99,17 @@ SIGNATURES = [
     ("sma_op_create_csc", c_int, [c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_void_p,
                                   c_int64, c_int64, ctypes.POINTER(c_void_p)]),
     ("sma_op_create_lap1d", c_int, [c_void_p, c_int64, ctypes.POINTER(c_void_p)]),
+    ("sma_op_create_anderson", c_int, [c_void_p, c_int64, c_void_p, c_double,
+                                       ctypes.POINTER(c_void_p)]),
+    ("sma_op_create_xxz", c_int, [c_void_p, c_int64, c_double, c_double, c_void_p,
+                                  ctypes.POINTER(c_void_p)]),
     ("sma_op_create_matblock", c_int, [c_void_p, c_int64, MATBLOCK_FN, c_void_p,
                                        ctypes.POINTER(c_void_p)]),
     ("sma_op_destroy", c_int, [c_void_p]),
     ("sma_op_info", c_int, [c_void_p, ctypes.POINTER(c_int64), ctypes.POINTER(c_int64)]),
     ("sma_gershgorin_bounds", c_int, [c_void_p, ctypes.POINTER(c_double), ctypes.POINTER(c_double)]),
+    ("sma_lanczos_bounds", c_int, [c_void_p, c_int64, c_int64, ctypes.POINTER(c_double),
+                                   ctypes.POINTER(c_double)]),
     ("sma_jackson_kernel", c_int, [c_int64, c_void_p]),
     ("sma_cheb_delta_coeffs", c_int, [c_double, c_int64, c_int64, c_void_p]),
     ("sma_cheb_window_coeffs", c_int, [c_double, c_double, c_int64, c_int64, c_void_p]),

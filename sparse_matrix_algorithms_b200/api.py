@@ -29,14 +29,16 @@ import scipy.sparse as sp
 from . import _lib as L
 
 __all__ = [
-    "Context", "context", "SparseOperator", "Lap1dOperator", "DeviceMatblock",
+    "Context", "context", "SparseOperator", "Lap1dOperator", "AndersonOperator", "XXZOperator",
+    "DeviceMatblock",
     "MatrixFreeRealSymOp", "chebyshev_poly_real_symm_sparse", "polfed", "gershgorin_bounds",
     "jackson_kernel", "cheb_delta_coeffs", "cheb_window_coeffs", "cheb_smooth_window_coeffs",
-    "build_coeffs", "apply_poly_block", "ArgumentError", "SMAError",
+    "build_coeffs", "apply_poly_block", "lanczos_bounds", "ArgumentError", "SMAError",
 ]
 
 ArgumentError = L.ArgumentError
 SMAError = L.SMAError
+_LIB = L  # for methods whose arguments are named L (lattice / chain length)
 
 
 # ====================================================================== context
@@ -141,6 +143,41 @@ class Lap1dOperator(_DeviceOp):
         self.handle = h
 
 
+class AndersonOperator(_DeviceOp):
+    """The 3D Anderson model of :func:`matrices.anderson3d` (same L, W, seed) as a device
+    stencil: no stored matrix, products bit-identical to the CSR matrix's."""
+
+    def __init__(self, L: int, W: float, seed: int, t: float = -1.0,
+                 ctx: Optional[Context] = None):
+        from .matrices import splitmix_uniform
+
+        self.ctx = ctx or context()
+        self.n = int(L) ** 3
+        eps = np.ascontiguousarray(W * (splitmix_uniform(seed, self.n) - 0.5))
+        h = ctypes.c_void_p()
+        _LIB.check(_LIB.load().sma_op_create_anderson(self.ctx.handle, int(L), eps.ctypes.data,
+                                                      float(t), ctypes.byref(h)))
+        self.handle = h
+
+
+class XXZOperator(_DeviceOp):
+    """The random-field XXZ chain of :func:`matrices.xxz_sz0` (same L, h, seed, J, Delta)
+    in the Sz = 0 sector as a device stencil (no stored matrix)."""
+
+    def __init__(self, L: int, h: float, seed: int, J: float = 1.0, Delta: float = 1.0,
+                 ctx: Optional[Context] = None):
+        from .matrices import splitmix_uniform
+        from math import comb
+
+        self.ctx = ctx or context()
+        self.n = comb(int(L), int(L) // 2)
+        field = np.ascontiguousarray(h * (2.0 * splitmix_uniform(seed, L) - 1.0))
+        hd = ctypes.c_void_p()
+        _LIB.check(_LIB.load().sma_op_create_xxz(self.ctx.handle, int(L), float(J), float(Delta),
+                                                 field.ctypes.data, ctypes.byref(hd)))
+        self.handle = hd
+
+
 class DeviceMatblock(_DeviceOp):
     """Matrix-free operator from a device block callback.
 
@@ -190,7 +227,7 @@ class MatrixFreeRealSymOp:
 
 
 def _as_device_op(n: int, f) -> _DeviceOp:
-    if isinstance(f, (SparseOperator, Lap1dOperator, DeviceMatblock)):
+    if isinstance(f, _DeviceOp):
         if f.n != n:
             raise ArgumentError(L.SMA_ERR_ARG, f"operator dimension {f.n} != n = {n}")
         return f
@@ -261,6 +298,16 @@ def gershgorin_bounds(A):
     return _resolve_sparse(A).gershgorin_bounds()
 
 
+def lanczos_bounds(A, steps: int = 60, seed: int = 7):
+    """Spectral bounds from ``steps`` GPU Lanczos steps (an extension of the reference,
+    which has only Gershgorin bounds); clipped to the Gershgorin interval for matrices."""
+    op = _op_of(A)
+    lo, hi = ctypes.c_double(), ctypes.c_double()
+    L.check(L.load().sma_lanczos_bounds(op.handle, int(steps), int(seed), ctypes.byref(lo),
+                                        ctypes.byref(hi)))
+    return lo.value, hi.value
+
+
 # ====================================================================== the filter
 def apply_poly_block(A, Q: np.ndarray, coeffs, smin: float, smax: float,
                      precision: str = "fp64") -> np.ndarray:
@@ -281,7 +328,7 @@ def apply_poly_block(A, Q: np.ndarray, coeffs, smin: float, smax: float,
 def _op_of(A) -> _DeviceOp:
     if isinstance(A, MatrixFreeRealSymOp):
         return A.device_op
-    if isinstance(A, (SparseOperator, Lap1dOperator, DeviceMatblock)):
+    if isinstance(A, _DeviceOp):
         return A
     return _resolve_sparse(A)
 
@@ -313,7 +360,7 @@ def chebyshev_poly_real_symm_sparse(A, *args, smin=None, smax=None, sigma: float
                                     jackson: bool = True, debug: bool = False,
                                     two_hit: bool = True, seed: int = 1,
                                     window_type="step", matblock=None, precision: str = "fp64",
-                                    stats: Optional[dict] = None, **kw):
+                                    lock: bool = False, stats: Optional[dict] = None, **kw):
     """Chebyshev-filtered subspace iteration.
 
     ``chebyshev_poly_real_symm_sparse(A, emin, emax; ...)`` with a sparse matrix (or
@@ -325,7 +372,9 @@ def chebyshev_poly_real_symm_sparse(A, *args, smin=None, smax=None, sigma: float
     ``two_hit`` rule (``chebyshev_subspace_iteration.jl:771-848``).
 
     Returns ``(lam, X, res)`` sorted by lambda, with absolute residuals.  ``sigma`` may
-    also be passed as ``σ``; ``precision="fp32"`` runs the filter in FP32.
+    also be passed as ``σ``.  Extensions: ``precision="fp32"`` runs the filter in FP32,
+    ``"mixed"`` in FP32 until the residuals stop improving and in FP64 after that;
+    ``lock=True`` locks converged pairs (stopping on the matrix-free ``two_hit`` rule).
     """
     if "σ" in kw:
         sigma = kw.pop("σ")
@@ -333,6 +382,8 @@ def chebyshev_poly_real_symm_sparse(A, *args, smin=None, smax=None, sigma: float
         raise TypeError(f"unexpected keyword arguments {sorted(kw)}")
     if isinstance(A, MatrixFreeRealSymOp):
         op, (emin, emax), mf = A.device_op, args, True
+    elif isinstance(A, _DeviceOp) and not isinstance(A, SparseOperator):  # device stencil
+        op, (emin, emax), mf = A, args, True
     elif sp.issparse(A) or isinstance(A, SparseOperator):
         if matblock is not None:
             raise TypeError("matblock is a keyword of the matrix-free overload")
@@ -351,6 +402,7 @@ def chebyshev_poly_real_symm_sparse(A, *args, smin=None, smax=None, sigma: float
     o.window_type = _window(window_type)
     o.matrix_free = int(mf)
     o.precision = L.PRECISIONS[precision]
+    o.lock = int(bool(lock))
     h = ctypes.c_void_p()
     L.check(L.load().sma_cheb_solve(op.handle, float(emin), float(emax), ctypes.byref(o),
                                     ctypes.byref(h)))
@@ -379,7 +431,7 @@ def polfed(A, *args, s: int = 8, smin=None, smax=None, sigma: float = 0.0,
         raise TypeError(f"unexpected keyword arguments {sorted(kw)}")
     if isinstance(A, MatrixFreeRealSymOp):
         op, (nev, degree) = A.device_op, args
-    elif sp.issparse(A) or isinstance(A, (SparseOperator, Lap1dOperator, DeviceMatblock)):
+    elif sp.issparse(A) or isinstance(A, _DeviceOp):
         op, (nev, degree) = _op_of(A), args
     else:
         n, nev, degree = args

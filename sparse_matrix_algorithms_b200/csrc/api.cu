@@ -55,6 +55,7 @@ void free_op(sma_op *op) {
   if (op->colind) cudaFree(op->colind);
   if (op->val64) cudaFree(op->val64);
   if (op->val32) cudaFree(op->val32);
+  free_stencil_arrays(op);
   delete op;
 }
 
@@ -431,7 +432,8 @@ int sma_cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts *op
     *out = nullptr;
     sma_cheb_opts o;
     if (opts) o = *opts; else sma_cheb_opts_default(&o);
-    require(o.precision == SMA_PREC_FP64 || o.precision == SMA_PREC_FP32, SMA_ERR_ARG, "unknown precision");
+    require(o.precision == SMA_PREC_FP64 || o.precision == SMA_PREC_FP32 ||
+                o.precision == SMA_PREC_MIXED, SMA_ERR_ARG, "unknown precision");
     if (o.has_bounds) check_bounds(o.smin, o.smax);
     DeviceGuard g(op->ctx->device);
     *out = cheb_solve(op, emin, emax, o);
@@ -446,7 +448,8 @@ int sma_polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polfed_o
     *out = nullptr;
     sma_polfed_opts o;
     if (opts) o = *opts; else sma_polfed_opts_default(&o);
-    require(o.precision == SMA_PREC_FP64 || o.precision == SMA_PREC_FP32, SMA_ERR_ARG, "unknown precision");
+    require(o.precision == SMA_PREC_FP64 || o.precision == SMA_PREC_FP32 ||
+                o.precision == SMA_PREC_MIXED, SMA_ERR_ARG, "unknown precision");
     if (o.has_bounds) check_bounds(o.smin, o.smax);
     DeviceGuard g(op->ctx->device);
     *out = polfed_solve(op, nev, degree, o);

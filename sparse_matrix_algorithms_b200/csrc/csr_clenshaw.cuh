@@ -139,8 +139,72 @@ staged_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
   }
 }
 
+// ASYNC family: every thread moves exactly 16 bytes (V = 16/sizeof(T) elements) of each
+// neighbour row it needs with cp.async (global -> shared, asynchronous), for up to NB
+// neighbours at a time plus the epilogue rows of Q, B1 and B2, then waits for its own
+// copies only and computes from shared memory.  All of a row's gathers are in flight at
+// once without holding registers, so a row costs one memory latency.  Each thread reads
+// back only the chunks it copied itself, so no barrier is needed.  CTAs are 128 threads;
+// shared memory per CTA is (NB + 3) * 128 * 16 bytes (22.5 KB for NB = 8, 38.9 KB for 16).
+constexpr int kAsyncThreads = 128;
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+template <typename T, int G, int NB, bool HQ, bool HS, bool HB>
+__global__ void __launch_bounds__(kAsyncThreads)
+async_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
+             const T *__restrict__ val, int64_t n, int b, const T *__restrict__ Q, int64_t ldq,
+             const T *__restrict__ B1, const T *__restrict__ B2, int64_t ldb,
+             T *__restrict__ out, int64_t ldo, T ck, T alpha, T beta) {
+  constexpr int V = 16 / (int)sizeof(T);
+  constexpr int kRows = kAsyncThreads / G;
+  __shared__ uint4 buf[NB + 3][kAsyncThreads];  // slot-major: a warp's copies are contiguous
+  const int64_t row = (int64_t)blockIdx.x * kRows + threadIdx.x / G;
+  if (row >= n) return;
+  const int tid = threadIdx.x;
+  const int lane = tid % G;
+  const int start = __ldg(rowptr + row);
+  const int end = __ldg(rowptr + row + 1);
+  for (int c0 = lane * V; c0 < b; c0 += G * V) {
+    if constexpr (HQ) cp_async16(&buf[NB][tid], Q + row * ldq + c0);
+    if constexpr (HS) cp_async16(&buf[NB + 1][tid], B1 + row * ldb + c0);
+    if constexpr (HB) cp_async16(&buf[NB + 2][tid], B2 + row * ldb + c0);
+    T acc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] = T(0);
+    for (int j0 = start; j0 < end; j0 += NB) {
+      const int cnt = min(NB, end - j0);
+      for (int u = 0; u < cnt; ++u)
+        cp_async16(&buf[u][tid], B1 + (int64_t)__ldg(colind + j0 + u) * ldb + c0);
+      cp_async_wait_all();
+      for (int u = 0; u < cnt; ++u) {
+        const T a = __ldg(val + j0 + u);
+        const T *x = reinterpret_cast<const T *>(&buf[u][tid]);
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[v] = fma(a, x[v], acc[v]);
+      }
+    }
+    cp_async_wait_all();  // epilogue rows of an empty row
+    T q[V], s[V], t[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      if constexpr (HQ) q[v] = reinterpret_cast<const T *>(&buf[NB][tid])[v];
+      if constexpr (HS) s[v] = reinterpret_cast<const T *>(&buf[NB + 1][tid])[v];
+      if constexpr (HB) t[v] = reinterpret_cast<const T *>(&buf[NB + 2][tid])[v];
+    }
+    epilogue<T, V, HQ, HS, HB>(out + row * ldo + c0, acc, q, s, t, ck, alpha, beta);
+  }
+}
+
 // ------------------------------------------------------------------ configurations
-// Encoded as fam | V << 4 | G << 8 | U << 16.
+// Encoded as fam | V << 4 | G << 8 | U << 16 (for the ASYNC family U is NB).
 inline int enc(int fam, int V, int G, int U) { return fam | (V << 4) | (G << 8) | (U << 16); }
 inline int fam_of(int c) { return c & 15; }
 inline int v_of(int c) { return (c >> 4) & 15; }
@@ -179,9 +243,38 @@ void launch_one(int fam, const Args<T> &a) {
   SMA_CHECK_LAUNCH();
 }
 
+template <typename T, int G, int NB, bool HQ, bool HS, bool HB>
+void launch_async(const Args<T> &a) {
+  const T *val;
+  if constexpr (sizeof(T) == 8) val = (const T *)a.op->val64;
+  else val = (const T *)a.op->val32;
+  constexpr int kRows = kAsyncThreads / G;
+  const unsigned grid = (unsigned)((a.op->n + kRows - 1) / kRows);
+  async_kernel<T, G, NB, HQ, HS, HB><<<grid, kAsyncThreads, 0, a.st>>>(
+      a.op->rowptr, a.op->colind, val, a.op->n, (int)a.b, a.Q, a.ldq, a.B1, a.B2, a.ldb, a.out,
+      a.ldo, (T)a.ck, (T)a.alpha, (T)a.beta);
+  SMA_CHECK_LAUNCH();
+}
+
 template <typename T, int V, bool HQ, bool HS, bool HB>
 void launch_v(int c, const Args<T> &a) {
   const int fam = fam_of(c);
+  if (fam == 2) {
+    if constexpr (V * sizeof(T) == 16) {
+      switch (g_of(c) * 100 + u_of(c)) {
+        case 408: return launch_async<T, 4, 8, HQ, HS, HB>(a);
+        case 416: return launch_async<T, 4, 16, HQ, HS, HB>(a);
+        case 808: return launch_async<T, 8, 8, HQ, HS, HB>(a);
+        case 816: return launch_async<T, 8, 16, HQ, HS, HB>(a);
+        case 1608: return launch_async<T, 16, 8, HQ, HS, HB>(a);
+        case 1616: return launch_async<T, 16, 16, HQ, HS, HB>(a);
+        case 3208: return launch_async<T, 32, 8, HQ, HS, HB>(a);
+        case 3216: return launch_async<T, 32, 16, HQ, HS, HB>(a);
+        default: break;
+      }
+    }
+    throw Error(SMA_ERR_INTERNAL, "bad asynchronous CSR kernel configuration");
+  }
   switch (g_of(c) * 100 + u_of(c)) {
     case 404: return launch_one<T, V, 4, 4, HQ, HS, HB>(fam, a);
     case 408: return launch_one<T, V, 4, 8, HQ, HS, HB>(fam, a);
@@ -248,6 +341,14 @@ void step(const Args<T> &a) {
           tu.cands.push_back(enc(fam, V, G, 4));
         }
       }
+    if (vmax * (int)sizeof(T) >= 16) {  // the ASYNC family moves 16-byte chunks
+      const int V = 16 / (int)sizeof(T);
+      const int64_t lanes = (a.b + V - 1) / V;
+      const int g0 = lanes <= 4 ? 4 : lanes <= 8 ? 8 : lanes <= 16 ? 16 : 32;
+      tu.cands.push_back(enc(2, V, g0, 8));
+      tu.cands.push_back(enc(2, V, g0, 16));
+      if (g0 >= 8) tu.cands.push_back(enc(2, V, g0 / 2, 8));
+    }
     if (!op->ctx->autotune || op->n < 20000) {
       tu.chosen = tu.cands[0];
       return launch_cfg<T, HQ, HS, HB>(tu.chosen, a);
@@ -281,7 +382,8 @@ void step(const Args<T> &a) {
     fprintf(stderr, "sma autotune: %s n=%lld b=%lld ld=%lld variant=%d%d%d ->", sizeof(T) == 8 ? "fp64" : "fp32",
             (long long)op->n, (long long)a.b, (long long)a.ldb, (int)HQ, (int)HS, (int)HB);
     for (size_t i = 0; i < ncand; ++i)
-      fprintf(stderr, " %s%s/V%d/G%d/U%d=%.1fus", i == w ? "*" : "", fam_of(tu.cands[i]) ? "staged" : "direct",
+      fprintf(stderr, " %s%s/V%d/G%d/U%d=%.1fus", i == w ? "*" : "",
+              fam_of(tu.cands[i]) == 2 ? "async" : fam_of(tu.cands[i]) ? "staged" : "direct",
               v_of(tu.cands[i]), g_of(tu.cands[i]), u_of(tu.cands[i]), 1e3 * best[i]);
     fprintf(stderr, "\n");
   }

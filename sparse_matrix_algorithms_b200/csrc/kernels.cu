@@ -23,14 +23,22 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Each stencil functor has prepare(row), the per-row work done once, and product(prep, ...)
+// for one column pass: acc += (A B1)[row, c0:c0+V].
+//
 // tridiag(-1,2,-1) stencil, evaluated as the reference's lap1d_matblock!
 // (polfed.jl:1209-1219): Y[1]=2X[1]-X[2]; Y[i]=-X[i-1]+2X[i]-X[i+1]; Y[n]=-X[n-1]+2X[n].
 template <typename T>
 struct Lap1dRows {
   int64_t n;
+  struct Prep {
+    int64_t row;
+  };
+  __device__ __forceinline__ Prep prepare(int64_t row) const { return {row}; }
   template <int V>
-  __device__ __forceinline__ void product(int64_t row, const T *__restrict__ B1, int64_t ldb,
+  __device__ __forceinline__ void product(const Prep &p, const T *__restrict__ B1, int64_t ldb,
                                           int c0, T (&acc)[V]) const {
+    const int64_t row = p.row;
     T xm[V], x0[V], xp[V];
     ldv<T, V>(B1 + row * ldb + c0, x0);
     if (row == 0) {
@@ -50,6 +58,120 @@ struct Lap1dRows {
   }
 };
 
+// 3D Anderson model on an L^3 periodic lattice, row i = x + L*(y + L*z): diag[i] on the
+// diagonal and `hop` at the six neighbours x+-1, y+-1, z+-1.  The seven terms are sorted by
+// column with a 16-comparator sorting network and accumulated in that order -- the order
+// of the stored matrix's CSR row -- so the stencil and the CSR kernel give bit-identical
+// products.  Needs L >= 3 (six distinct neighbours).
+template <typename T>
+struct AndersonRows {
+  int64_t L;
+  const double *__restrict__ diag;
+  T hop;
+  // sorted columns (int32: n < 2^31) and the sorted position of the diagonal entry
+  struct Prep {
+    int c[7];
+    int dpos;
+    T d;
+  };
+  __device__ __forceinline__ Prep prepare(int64_t row64) const {
+    const int row = (int)row64, l = (int)L, l2 = l * l;
+    const int x = row % l, y = (row / l) % l, z = row / l2;
+    int r0 = row, r1 = x + 1 == l ? row - (l - 1) : row + 1, r2 = x == 0 ? row + (l - 1) : row - 1;
+    int r3 = y + 1 == l ? row - (l - 1) * l : row + l, r4 = y == 0 ? row + (l - 1) * l : row - l;
+    int r5 = z + 1 == l ? row - (l - 1) * l2 : row + l2, r6 = z == 0 ? row + (l - 1) * l2 : row - l2;
+#define SMA_CS(i, j)         \
+  if (r##i > r##j) {         \
+    const int tr = r##i;     \
+    r##i = r##j;             \
+    r##j = tr;               \
+  }
+    SMA_CS(0, 6) SMA_CS(2, 3) SMA_CS(4, 5) SMA_CS(0, 2) SMA_CS(1, 4) SMA_CS(3, 6)
+    SMA_CS(0, 1) SMA_CS(2, 5) SMA_CS(3, 4) SMA_CS(1, 2) SMA_CS(4, 6) SMA_CS(2, 3)
+    SMA_CS(4, 5) SMA_CS(1, 2) SMA_CS(3, 4) SMA_CS(5, 6)
+#undef SMA_CS
+    Prep p{{r0, r1, r2, r3, r4, r5, r6}, 0, (T)__ldg(diag + row64)};
+#pragma unroll
+    for (int u = 0; u < 7; ++u)
+      if (p.c[u] == row) p.dpos = u;
+    return p;
+  }
+  template <int V>
+  __device__ __forceinline__ void product(const Prep &p, const T *__restrict__ B1, int64_t ldb,
+                                          int c0, T (&acc)[V]) const {
+    T xs[7][V];
+#pragma unroll
+    for (int u = 0; u < 7; ++u) ldv<T, V>(B1 + (int64_t)p.c[u] * ldb + c0, xs[u]);
+#pragma unroll
+    for (int u = 0; u < 7; ++u) {
+      const T a = u == p.dpos ? p.d : hop;
+#pragma unroll
+      for (int v = 0; v < V; ++v) acc[v] = fma(a, xs[u][v], acc[v]);
+    }
+  }
+};
+
+// Random-field XXZ chain of length L in the Sz = 0 sector.  Row r is the basis state
+// s = states[r] (bit i = site i up); its index is its combinatorial rank
+// sum_j C(p_j, j) over its set bits p_1 < p_2 < ... .  Flipping the antiparallel bond
+// (i, i+1) moves one set bit by one position, which changes the rank by +-C(i, k), k the
+// number of set bits below i; the periodic bond (L-1, 0) re-ranks the flipped state.
+// Terms: diag[r] x_r, then `hop` (J/2) times each neighbour in bond order.
+template <typename T>
+struct XxzRows {
+  int L;
+  const double *__restrict__ diag;
+  const unsigned *__restrict__ states;
+  const int *__restrict__ binom;  // C(p, k) at binom[p*17 + k]
+  T hop;
+  struct Prep {
+    int64_t row, pcol;  // pcol: neighbour across the periodic bond, or -1
+    unsigned s;
+    T d;
+  };
+  __device__ __forceinline__ Prep prepare(int64_t row) const {
+    Prep p{row, -1, __ldg(states + row), (T)__ldg(diag + row)};
+    if (((p.s >> (L - 1)) ^ p.s) & 1u) {
+      unsigned t = p.s ^ (1u | (1u << (L - 1)));
+      int64_t col = 0;
+      for (int j = 1; t; ++j) {
+        col += __ldg(binom + (__ffs(t) - 1) * 17 + j);
+        t &= t - 1;
+      }
+      p.pcol = col;
+    }
+    return p;
+  }
+  template <int V>
+  __device__ __forceinline__ void product(const Prep &p, const T *__restrict__ B1, int64_t ldb,
+                                          int c0, T (&acc)[V]) const {
+    const int64_t row = p.row;
+    const unsigned s = p.s;
+    T x[V];
+    ldv<T, V>(B1 + row * ldb + c0, x);
+    const T d = p.d;
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] = fma(d, x[v], acc[v]);
+    int k = 0;
+    for (int i = 0; i + 1 < L; ++i) {
+      const unsigned bi = (s >> i) & 1u;
+      if (bi != ((s >> (i + 1)) & 1u)) {
+        const int delta = __ldg(binom + i * 17 + k);
+        const int64_t col = bi ? row + delta : row - delta;
+        ldv<T, V>(B1 + col * ldb + c0, x);
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[v] = fma(hop, x[v], acc[v]);
+      }
+      k += (int)bi;
+    }
+    if (p.pcol >= 0) {
+      ldv<T, V>(B1 + p.pcol * ldb + c0, x);
+#pragma unroll
+      for (int v = 0; v < V; ++v) acc[v] = fma(hop, x[v], acc[v]);
+    }
+  }
+};
+
 // ------------------------------------------------------------------ stencil Clenshaw step
 template <typename T, int V, int G, bool HAS_Q, bool HAS_SELF, bool HAS_B2, typename Rows>
 __global__ void __launch_bounds__(kThreads)
@@ -60,15 +182,16 @@ stencil_step_kernel(Rows rows, int64_t n, int b, const T *__restrict__ Q, int64_
   const int lane = threadIdx.x % G;
   for (int64_t row = (int64_t)blockIdx.x * kRows + threadIdx.x / G; row < n;
        row += (int64_t)gridDim.x * kRows) {
+    const auto prep = rows.prepare(row);
     for (int c0 = lane * V; c0 < b; c0 += G * V) {
-      T acc[V];
-#pragma unroll
-      for (int v = 0; v < V; ++v) acc[v] = T(0);
-      rows.template product<V>(row, B1, ldb, c0, acc);
-      T q[V], s[V], t[V], r[V];
+      T acc[V], q[V], s[V], t[V], r[V];
+      // epilogue operands first, so that their latency overlaps the neighbour gathers
       if constexpr (HAS_Q) ldv<T, V>(Q + row * ldq + c0, q);
       if constexpr (HAS_SELF) ldv<T, V>(B1 + row * ldb + c0, s);
       if constexpr (HAS_B2) ldv<T, V>(B2 + row * ldb + c0, t);
+#pragma unroll
+      for (int v = 0; v < V; ++v) acc[v] = T(0);
+      rows.template product<V>(prep, B1, ldb, c0, acc);
 #pragma unroll
       for (int v = 0; v < V; ++v) {
         T x = alpha * acc[v];
@@ -411,6 +534,15 @@ void launch_clenshaw_step(const sma_op *op, cudaStream_t st, int64_t b, const T 
     csr_clenshaw_step<T>(op, st, b, Q, ldq, B1, B2, ldb, out, ldo, ck, alpha, beta, has_self);
   } else if (op->kind == OP_LAP1D) {
     Lap1dRows<T> rows{op->n};
+    dispatch_flags<T>(rows, st, op->n, b, Q, ldq, B1, B2, ldb, out, ldo, ck, alpha, beta, has_self);
+    SMA_CHECK_LAUNCH();
+  } else if (op->kind == OP_ANDERSON) {
+    AndersonRows<T> rows{op->stencil.L, op->stencil.diag, (T)op->stencil.hop};
+    dispatch_flags<T>(rows, st, op->n, b, Q, ldq, B1, B2, ldb, out, ldo, ck, alpha, beta, has_self);
+    SMA_CHECK_LAUNCH();
+  } else if (op->kind == OP_XXZ) {
+    XxzRows<T> rows{op->stencil.L, op->stencil.diag, op->stencil.states, op->stencil.binom,
+                    (T)op->stencil.hop};
     dispatch_flags<T>(rows, st, op->n, b, Q, ldq, B1, B2, ldb, out, ldo, ck, alpha, beta, has_self);
     SMA_CHECK_LAUNCH();
   } else {

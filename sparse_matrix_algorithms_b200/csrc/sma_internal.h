@@ -94,7 +94,17 @@ struct sma_ctx {
   bool autotune = true;  // SMA_AUTOTUNE=0 in the environment turns the kernel autotuner off
 };
 
-enum op_kind { OP_CSR = 0, OP_LAP1D = 1, OP_MATBLOCK = 2 };
+enum op_kind { OP_CSR = 0, OP_LAP1D = 1, OP_MATBLOCK = 2, OP_ANDERSON = 3, OP_XXZ = 4 };
+
+// Data of the matrix-free model stencils (kernels.cu): the 3D Anderson model on an L^3
+// periodic lattice and the XXZ chain in its Sz = 0 sector.
+struct sma_stencil {
+  int L = 0;                   // lattice / chain length
+  double hop = 0.0;            // Anderson hopping t, or the XXZ flip amplitude J/2
+  double *diag = nullptr;      // n on-site energies / diagonal entries (device)
+  unsigned *states = nullptr;  // XXZ: basis state (bit string) of each row (device)
+  int *binom = nullptr;        // XXZ: C(p, k) for p < 32, k <= 16, row-major 32 x 17 (device)
+};
 
 struct sma_op {
   sma_ctx *ctx = nullptr;
@@ -114,6 +124,8 @@ struct sma_op {
   void *user = nullptr;
   // autotuned CSR kernel configurations
   std::map<uint64_t, sma::CsrTune> tuned;
+  // matrix-free model stencils
+  sma_stencil stencil;
 };
 
 namespace sma {
@@ -210,6 +222,8 @@ void launch_gather_columns_rm(cudaStream_t st, int64_t n, int64_t k, const doubl
                               int64_t lds, const int64_t *idx, double *dst, int64_t ldd);
 // Gershgorin partial bounds of a CSR matrix
 void gershgorin_device(const sma_op *op, double *smin, double *smax);
+// Device arrays of a model stencil operator (stencils.cu)
+void free_stencil_arrays(sma_op *op);
 // Exact symmetry and sortedness check; returns 0 ok, 1 unsorted, 2 non-symmetric
 int check_csr_device(const sma_op *op);
 // In-place shift of the diagonal of a k x k column-major matrix

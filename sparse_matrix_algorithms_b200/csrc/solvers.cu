@@ -88,10 +88,20 @@ struct Filter {
   ClenshawWork<float> w32;
   DevBuf<float> q32, y32;
   FilterCount total;
+  int64_t columns = 0;     // sum of the block widths filtered
+  bool fp64_phase = false;  // MIXED: set once the FP32 phase has ended
+
+  bool in_fp32() const {
+    return precision == SMA_PREC_FP32 || (precision == SMA_PREC_MIXED && !fp64_phase);
+  }
+
+  int64_t fp32_calls = 0;
 
   void run(const double *Q, int64_t ldq, double *Y, int64_t ldy, int64_t b) {
     FilterCount fc;
-    if (precision == SMA_PREC_FP32) {
+    columns += b;
+    if (in_fp32()) {
+      ++fp32_calls;
       const int64_t n = op->n;
       if (q32.count < (size_t)(n * b)) {
         q32.alloc(n * b, st);
@@ -157,6 +167,159 @@ sma_result *empty_result(sma_ctx *ctx, int64_t n) {
 
 }  // namespace
 
+// MIXED precision: the FP32 phase ends when the in-window residuals reach what FP32 filtering
+// can deliver (1e-6 of the spectral scale), when they stop improving (less than a factor 2
+// over the previous iteration), or -- for the sparse overload, which runs a fixed number of
+// iterations -- when only two iterations remain.  Iterations after that filter in FP64.
+namespace {
+
+void mixed_switch(Filter &flt, int64_t cnt, double maxres, double prev_maxres, double scale,
+                  bool last_two) {
+  const bool small = cnt > 0 && maxres < 1e-6 * scale;
+  const bool stalled = cnt > 0 && std::isfinite(prev_maxres) && maxres > 0.5 * prev_maxres;
+  if (small || stalled || last_two) flt.fp64_phase = true;
+}
+
+
+// Chebyshev subspace iteration with locking (sma_cheb_opts.lock = 1, matrix-free overload
+// semantics for termination): the in-window Ritz pairs whose residual is below tol are
+// moved to a locked set, the remaining Ritz vectors form the next (narrower) block, and
+// every filtered block is projected against the locked vectors (two classical Gram-Schmidt
+// passes) before its orthonormalization -- the reference's append_locked!
+// (chebyshev_subspace_iteration.jl:282-290) put to use.
+sma_result *cheb_solve_locked(sma_op *op, double emin, double emax, const sma_cheb_opts &o,
+                              int64_t m0, double smin, double smax, Filter &flt, sma_stats &stats,
+                              std::chrono::steady_clock::time_point t0, int64_t launches0) {
+  sma_ctx *ctx = op->ctx;
+  cudaStream_t st = ctx->stream;
+  const int64_t n = op->n;
+  Dense dn(ctx);
+  PhaseClock clk(st);
+  DevBuf<double> Q(n * m0, st), Y(n * m0, st), X(n * m0, st), Xlock(n * m0, st),
+      Aq(m0 * m0, st), C(m0 * m0, st), lam_d(m0, st), res_d(m0, st), scratch;
+  launch_randn(st, n, m0, (uint64_t)o.seed, Q.p, m0);
+  std::vector<double> lam, res, lam_lock, res_lock;
+  int64_t m = m0, nlock = 0, it = 0;
+  bool prev_ok = false;
+  double prev_maxres = INFINITY;
+  for (it = 1; it <= o.maxiter && m > 0; ++it) {
+    const bool fp32_iteration = flt.in_fp32();
+    clk.mark(PH_FILTER);
+    flt.run(Q.p, m0, Y.p, m0, m);
+    clk.mark(PH_ORTH);
+    for (int pass = 0; pass < 2 && nlock > 0; ++pass) {  // Y -= Xlock (Xlock' Y)
+      dn.gram(n, nlock, m, Xlock.p, m0, Y.p, m0, C.p, m0);
+      dn.mul_small(n, nlock, m, Xlock.p, m0, C.p, m0, Y.p, m0, -1.0, 1.0);
+    }
+    std::swap(Q.p, Y.p);
+    orthonormalize(ctx, n, m, Q.p, m0, false, 0.0, nullptr, &stats.qr_fallbacks);
+    clk.mark(PH_RR);
+    op_apply(op, st, Q.p, m0, Y.p, m0, m);
+    dn.gram(n, m, m, Q.p, m0, Y.p, m0, Aq.p, m);
+    dn.syevd(m, Aq.p, m, lam_d.p, true);
+    dn.mul_small(n, m, m, Q.p, m0, Aq.p, m, X.p, m0, 1.0, 0.0);
+    op_apply(op, st, X.p, m0, Y.p, m0, m);
+    column_reduce(st, 1, n, m, X.p, m0, Y.p, m0, lam_d.p, res_d.p, scratch);
+    clk.close();
+    lam = dev_to_host(st, lam_d.p, m);
+    res = dev_to_host(st, res_d.p, m);
+    // convergence over locked + active pairs (chebyshev_subspace_iteration.jl:817-836)
+    int64_t cnt = nlock;
+    double maxres = nlock ? *std::max_element(res_lock.begin(), res_lock.end()) : -INFINITY;
+    for (int64_t j = 0; j < m; ++j)
+      if (lam[j] >= emin && lam[j] <= emax && res[j] < o.res_gate) {
+        ++cnt;
+        maxres = std::max(maxres, res[j]);
+      }
+    if (cnt == 0) maxres = INFINITY;
+    if (o.debug) {
+      printf("it=%lld inside=%lld locked=%lld maxres=%.3e\n", (long long)it, (long long)cnt,
+             (long long)nlock, maxres);
+      fflush(stdout);
+    }
+    if (o.precision == SMA_PREC_MIXED && fp32_iteration)
+      mixed_switch(flt, cnt, maxres, prev_maxres, std::max(std::fabs(smin), std::fabs(smax)), false);
+    prev_maxres = maxres;
+    const bool ok = cnt > 0 && maxres < o.tol && !fp32_iteration;
+    if (o.two_hit ? (ok && (it == 1 || prev_ok)) : ok) {
+      ++it;
+      break;
+    }
+    prev_ok = ok;
+    if (fp32_iteration) continue;  // lock only pairs converged in FP64 arithmetic
+    // lock the converged in-window pairs; the other Ritz vectors form the next block
+    std::vector<int64_t> keep, lockj;
+    for (int64_t j = 0; j < m; ++j)
+      (lam[j] >= emin && lam[j] <= emax && res[j] < o.tol ? lockj : keep).push_back(j);
+    if (lockj.empty()) {
+      std::swap(Q.p, X.p);  // next block: the Ritz vectors
+      continue;
+    }
+    {
+      DevBuf<int64_t> d = upload_idx(st, lockj);
+      launch_gather_columns_rm(st, n, (int64_t)lockj.size(), X.p, m0, d.p, Xlock.p + nlock, m0);
+    }
+    for (int64_t j : lockj) {
+      lam_lock.push_back(lam[j]);
+      res_lock.push_back(res[j]);
+    }
+    nlock += (int64_t)lockj.size();
+    m = (int64_t)keep.size();
+    if (m > 0) {
+      DevBuf<int64_t> d = upload_idx(st, keep);
+      launch_gather_columns_rm(st, n, m, X.p, m0, d.p, Q.p, m0);
+    }
+  }
+  double ph[PH_COUNT] = {0, 0, 0};
+  clk.totals(ph);
+  stats.iterations = it - 1;
+  stats.basis_dim = m0;
+  stats.spmm_steps = flt.total.steps;
+  stats.spmm_columns = flt.columns * (int64_t)(flt.coeffs.size() > 1 ? flt.coeffs.size() - 1 : 1);
+  stats.filter_bytes = flt.total.bytes;
+  stats.fp32_filter_calls = flt.fp32_calls;
+  stats.locked = nlock;
+  stats.filter_ms = ph[PH_FILTER];
+  stats.orth_ms = ph[PH_ORTH];
+  stats.rr_ms = ph[PH_RR];
+  // selection over locked and active pairs, sorted by eigenvalue
+  const double gate = std::max(o.res_gate, 10.0 * o.tol);
+  std::vector<double> lam_all = lam_lock, res_all = res_lock;
+  std::vector<int64_t> idx;
+  for (int64_t j = 0; j < nlock; ++j) idx.push_back(j);
+  if (m > 0)
+    for (int64_t j = 0; j < (int64_t)lam.size(); ++j)
+      if (lam[j] >= emin && lam[j] <= emax && res[j] < gate) {
+        lam_all.push_back(lam[j]);
+        res_all.push_back(res[j]);
+        idx.push_back(nlock + j);
+      }
+  sma_result *r;
+  if (idx.empty()) {
+    r = empty_result(ctx, n);
+  } else {
+    // side by side: locked vectors, then the active Ritz vectors
+    DevBuf<double> Xall(n * (nlock + std::max<int64_t>(m, 0)) + 1, st);
+    const int64_t w = nlock + std::max<int64_t>(m, 0);
+    if (nlock)
+      SMA_CUDA(cudaMemcpy2DAsync(Xall.p, w * sizeof(double), Xlock.p, m0 * sizeof(double),
+                                 nlock * sizeof(double), n, cudaMemcpyDeviceToDevice, st));
+    if (m > 0)
+      SMA_CUDA(cudaMemcpy2DAsync(Xall.p + nlock, w * sizeof(double), X.p, m0 * sizeof(double),
+                                 m * sizeof(double), n, cudaMemcpyDeviceToDevice, st));
+    std::vector<double> lsel(lam_all.size());
+    for (size_t i = 0; i < lam_all.size(); ++i) lsel[i] = lam_all[i];
+    const std::vector<int64_t> p = stable_argsort(lsel);
+    r = make_result(ctx, n, Xall.p, w, take(idx, p), take(lam_all, p), take(res_all, p));
+  }
+  stats.total_ms = ms_since(t0);
+  stats.kernel_launches = g_kernel_launches.load() - launches0;
+  r->stats = stats;
+  return r;
+}
+
+}  // namespace
+
 // ====================================================================== Chebyshev
 // chebyshev_poly_real_symm_sparse, chebyshev_subspace_iteration.jl:667-757 (sparse
 // overload, matrix_free = 0) and 771-848 (matrix-free overload, matrix_free = 1).
@@ -208,21 +371,24 @@ sma_result *cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts
              mf ? "" : "; provide better spectral bounds");
     throw Error(SMA_ERR_INTERVAL, buf);
   }
-  if (o.precision == SMA_PREC_FP32) {
+  if (o.precision != SMA_PREC_FP64) {
     require(op->kind != OP_MATBLOCK, SMA_ERR_ARG, "FP32 filtering needs a device operator");
     ensure_fp32_values(op);
   }
   Filter flt{op, st, build_coeffs(degree, smin, smax, o.sigma, emin, emax, o.window_type, o.jackson != 0),
              smin, smax, o.precision};
+  if (o.lock) return cheb_solve_locked(op, emin, emax, o, m0, smin, smax, flt, stats, t0, launches0);
   Dense dn(ctx);
   PhaseClock clk(st);
   DevBuf<double> Q(n * m0, st), Y(n * m0, st), X(n * m0, st), Aq(m0 * m0, st), lam_d(m0, st),
       res_d(m0, st), scratch;
+  double prev_maxres = INFINITY;
   launch_randn(st, n, m0, (uint64_t)o.seed, Q.p, m0);  // Random.seed!(seed); Q=randn(n,m0)
   std::vector<double> lam, res;
   bool prev_ok = false;
   int64_t it = 0;
   for (it = 1; it <= o.maxiter; ++it) {
+    const bool fp32_iteration = flt.in_fp32();
     clk.mark(PH_FILTER);
     flt.run(Q.p, m0, Y.p, m0, m0);                         // Y = p(A_hat) Q
     clk.mark(PH_ORTH);
@@ -265,8 +431,12 @@ sma_result *cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts
       }
       fflush(stdout);
     }
+    if (o.precision == SMA_PREC_MIXED && fp32_iteration)
+      mixed_switch(flt, cnt, maxres, prev_maxres, std::max(std::fabs(smin), std::fabs(smax)),
+                   !mf && it >= o.maxiter - 2);
+    prev_maxres = maxres;
     if (mf) {  // chebyshev_subspace_iteration.jl:827-836
-      const bool ok = cnt > 0 && maxres < o.tol;
+      const bool ok = cnt > 0 && maxres < o.tol && !fp32_iteration;
       if (o.two_hit) {
         if (ok && (it == 1 || prev_ok)) {
           if (o.debug) { printf("converged\n"); fflush(stdout); }
@@ -287,6 +457,7 @@ sma_result *cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts
   stats.spmm_steps = flt.total.steps;
   stats.spmm_columns = flt.total.steps * m0;
   stats.filter_bytes = flt.total.bytes;
+  stats.fp32_filter_calls = flt.fp32_calls;
   stats.filter_ms = ph[PH_FILTER];
   stats.orth_ms = ph[PH_ORTH];
   stats.rr_ms = ph[PH_RR];
@@ -351,7 +522,7 @@ sma_result *polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polf
   require(o.s > 0 && o.s <= n, SMA_ERR_ARG, "block size s must be in 1..n");
   require(o.overextract >= 0 && o.extra_keep >= 0, SMA_ERR_ARG, "overextract and extra_keep must be nonnegative");
   const double smin = o.smin, smax = o.smax;
-  if (o.precision == SMA_PREC_FP32) {
+  if (o.precision != SMA_PREC_FP64) {
     require(op->kind != OP_MATBLOCK, SMA_ERR_ARG, "FP32 filtering needs a device operator");
     ensure_fp32_values(op);
   }
@@ -457,7 +628,9 @@ sma_result *polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polf
     double ph[PH_COUNT] = {0, 0, 0};
     clk.totals(ph);
     stats.spmm_steps = flt.total.steps;
+    stats.spmm_columns = flt.columns * (int64_t)(flt.coeffs.size() > 1 ? flt.coeffs.size() - 1 : 1);
     stats.filter_bytes = flt.total.bytes;
+    stats.fp32_filter_calls = flt.fp32_calls;
     stats.filter_ms = ph[PH_FILTER];
     stats.orth_ms = ph[PH_ORTH];
     stats.rr_ms = ph[PH_RR];
@@ -469,6 +642,23 @@ sma_result *polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polf
   if (idx_keep.empty()) {
     if (o.show_progress) { printf("m=%lld  inside=0  maxres=Inf\n", (long long)nb); fflush(stdout); }
     return finish(empty_result(ctx, n));
+  }
+  // MIXED: guard Ritz vectors for the FP64 polish, taken in theta order from the
+  // out-of-window columns of X before the refinement reuses X's storage. Without guards
+  // the polish converges at the ratio p(first outside)/p(window edge), which is close to 1.
+  DevBuf<double> guard;
+  int64_t ng = 0;
+  if (o.precision == SMA_PREC_MIXED) {
+    std::vector<int64_t> out;
+    const int64_t want = std::max<int64_t>(1, ((int64_t)idx_keep.size() + 1) / 2);
+    for (int64_t jj = 0; jj < m && (int64_t)out.size() < want; ++jj)
+      if (!(o.emin <= rs.lam[jj] && rs.lam[jj] <= o.emax)) out.push_back(jj);
+    ng = (int64_t)out.size();
+    if (ng > 0) {
+      guard.alloc(n * ng, st);
+      DevBuf<int64_t> d = upload_idx(st, out);
+      launch_gather_columns_rm(st, n, ng, X.p, m, d.p, guard.p, ng);
+    }
   }
   const int64_t npre = std::min<int64_t>((int64_t)res_keep.size(), nev + o.extra_keep);
   std::vector<int64_t> ps0 = stable_argsort(res_keep);
@@ -515,6 +705,57 @@ sma_result *polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polf
       return finish(empty_result(ctx, n));
     }
     Xfin = X.p;
+    ldfin = k;
+  }
+  DevBuf<double> Xpol;
+  if (o.precision == SMA_PREC_MIXED) {
+    // FP64 polish of an FP32-filtered basis: Chebyshev subspace iterations with the same
+    // filter in FP64 on the in-window candidates plus the guard vectors (orthonormalize,
+    // Rayleigh-Ritz with A, residuals), until the best min(nev, in-window) residuals are
+    // below tol; at most three passes.
+    flt.fp64_phase = true;
+    const int64_t kin = (int64_t)colmap.size();
+    const int64_t k = kin + ng;
+    Xpol.alloc(n * k, st);
+    DevBuf<double> Yp(n * k, st), Hp(k * k, st), mup(k, st), AXp(n * k, st);
+    {
+      DevBuf<int64_t> d = upload_idx(st, colmap);
+      launch_gather_columns_rm(st, n, kin, Xfin, ldfin, d.p, Yp.p, kin);
+      launch_copy_block<double, double>(st, n, kin, Yp.p, kin, Xpol.p, k);
+      if (ng > 0) launch_copy_block<double, double>(st, n, ng, guard.p, ng, Xpol.p + kin, k);
+    }
+    auto converged = [&] {
+      std::vector<double> r;
+      for (size_t i = 0; i < lamc.size(); ++i)
+        if (o.emin <= lamc[i] && lamc[i] <= o.emax) r.push_back(resc[i]);
+      if (r.empty()) return false;
+      std::sort(r.begin(), r.end());
+      return r[std::min<size_t>(nev, r.size()) - 1] < o.tol;
+    };
+    for (int pol = 0; pol < 3 && !converged(); ++pol) {
+      clk.mark(PH_FILTER);
+      flt.run(Xpol.p, k, Yp.p, k, k);
+      clk.mark(PH_RR);
+      orthonormalize(ctx, n, k, Yp.p, k, false, 0.0, nullptr, &stats.qr_fallbacks);
+      op_apply(op, st, Yp.p, k, AXp.p, k, k);
+      dn.gram(n, k, k, Yp.p, k, AXp.p, k, Hp.p, k);
+      dn.syevd(k, Hp.p, k, mup.p, true);
+      dn.mul_small(n, k, k, Yp.p, k, Hp.p, k, Xpol.p, k, 1.0, 0.0);
+      RitzSet rp = rayleigh(op, st, n, k, Xpol.p, k, AXp.p, lam_d, res_d, scratch);
+      clk.close();
+      lamc = rp.lam;
+      resc = rp.res;
+      stats.polish_iterations += 1;
+    }
+    // keep the in-window pairs, as the refinement does; without a polish pass lamc still
+    // describes the first kin columns of Xpol (the refined candidates)
+    std::vector<int64_t> in;
+    for (int64_t i = 0; i < (int64_t)lamc.size(); ++i)
+      if (o.emin <= lamc[i] && lamc[i] <= o.emax) in.push_back(i);
+    lamc = take(lamc, in);
+    resc = take(resc, in);
+    colmap = in;
+    Xfin = Xpol.p;
     ldfin = k;
   }
   const int64_t nkeep = std::min<int64_t>((int64_t)resc.size(), nev + o.extra_keep);

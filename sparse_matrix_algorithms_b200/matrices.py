@@ -219,8 +219,9 @@ def _canonical(A: sp.spmatrix) -> sp.csr_matrix:
     A = sp.csr_matrix(A, dtype=np.float64)
     A.sum_duplicates()
     A.sort_indices()
-    A.indices = A.indices.astype(np.int32)
-    A.indptr = A.indptr.astype(np.int64)
+    idx = np.int32 if A.nnz < 2**31 - 1 else np.int64  # scipy wants one index dtype
+    A.indices = A.indices.astype(idx)
+    A.indptr = A.indptr.astype(idx)
     return A
 
 
@@ -250,6 +251,47 @@ def load_csr(path: str) -> sp.csr_matrix:
         indices = np.frombuffer(f.read(4 * nnz), dtype="<i4")
         data = np.frombuffer(f.read(8 * nnz), dtype="<f8")
     return _canonical(sp.csr_matrix((data, indices, indptr), shape=(n, n)))
+
+
+def save_mtx(path: str, A: sp.spmatrix, comment: str = "") -> None:
+    """Write ``A`` in Matrix Market coordinate format: ``real symmetric`` (lower triangle,
+    1-based) when A == A^T, ``real general`` otherwise; values with 17 significant digits so
+    that a reader recovers every double exactly.  Julia reads it with
+    ``MatrixMarket.mmread``."""
+    A = _canonical(A)
+    n = A.shape[0]
+    sym = (abs(A - A.T)).nnz == 0
+    C = sp.tril(A).tocoo() if sym else A.tocoo()
+    order = np.lexsort((C.row, C.col))  # column-major entry order
+    with open(path, "w") as f:
+        f.write(f"%%MatrixMarket matrix coordinate real {'symmetric' if sym else 'general'}\n")
+        for line in comment.splitlines():
+            f.write(f"% {line}\n")
+        f.write(f"{n} {A.shape[1]} {C.nnz}\n")
+        for i, j, v in zip(C.row[order], C.col[order], C.data[order]):
+            f.write(f"{i + 1} {j + 1} {float(v)!r}\n")  # shortest round-trip repr
+
+
+def load_mtx(path: str) -> sp.csr_matrix:
+    """Read a Matrix Market coordinate file (``real``/``integer``, ``general`` or
+    ``symmetric``) into the canonical CSR form."""
+    with open(path) as f:
+        header = f.readline().split()
+        if len(header) < 5 or header[0] != "%%MatrixMarket" or header[2] != "coordinate":
+            raise ValueError(f"{path}: not a Matrix Market coordinate file")
+        symmetric = header[4].lower() == "symmetric"
+        line = f.readline()
+        while line.startswith("%"):
+            line = f.readline()
+        m, n, nnz = (int(x) for x in line.split())
+        data = np.loadtxt(f, ndmin=2) if nnz else np.zeros((0, 3))
+    i = data[:, 0].astype(np.int64) - 1
+    j = data[:, 1].astype(np.int64) - 1
+    v = data[:, 2].astype(np.float64)
+    if symmetric:
+        off = i != j
+        i, j, v = np.concatenate([i, j[off]]), np.concatenate([j, i[off]]), np.concatenate([v, v[off]])
+    return _canonical(sp.coo_matrix((v, (i, j)), shape=(m, n)).tocsr())
 
 
 def config_matrix(name: str) -> sp.csr_matrix:

@@ -61,6 +61,28 @@ def test_filter_fp64_matches_oracle(lib_built, name, b):
         assert np.abs(got - ref).max() <= 1e-12 * scale, (K, window)
 
 
+@pytest.mark.parametrize("name,b", [("anderson_L28", 8), ("anderson_L28", 32), ("xxz_L18", 32),
+                                    ("xxz_L18", 48), ("xxz_L18", 6)])
+def test_filter_all_autotuner_candidates_match_oracle(lib_built, name, b):
+    """Operators with n >= 20000 are autotuned online: the first 2 x (candidates) steps of
+    the recurrence each run a different kernel configuration (all three families), so
+    the result checks every configuration on real work."""
+    import sparse_matrix_algorithms_b200 as S
+
+    A = M.anderson3d(28, 16.5, 9) if name == "anderson_L28" else M.xxz_sz0(18, 5.0, 1)
+    smin, smax = _bounds(A)
+    op = S.SparseOperator(A)
+    Q = M.splitmix_normal(5, A.shape[0], b)
+    c = O.build_coeffs(90, smin, smax, 0.0, -0.3, 0.3, "step", True)
+    ref = O.apply_poly_block(A, Q, c, smin, smax)
+    for _ in range(2):  # tuning run, then the chosen configuration
+        got = S.apply_poly_block(op, Q, c, smin, smax)
+        assert np.abs(got - ref).max() <= 1e-12 * max(np.abs(ref).max(), np.abs(Q).max())
+    got32 = S.apply_poly_block(op, Q, c, smin, smax, precision="fp32")
+    got32 = S.apply_poly_block(op, Q, c, smin, smax, precision="fp32")
+    assert np.abs(got32 - ref).max() <= 2e-4 * np.abs(ref).max()
+
+
 @pytest.mark.parametrize("b", [1, 4, 6, 32, 96])
 def test_filter_fp32_close_to_oracle(lib_built, b):
     import sparse_matrix_algorithms_b200 as S
@@ -95,6 +117,42 @@ def test_lap1d_stencil_operator_matches_csr_oracle(lib_built):
         ref = O.apply_poly_block(M.lap1d(n), Q, c, 0.0, 4.0)
         got = S.apply_poly_block(op, Q, c, 0.0, 4.0)
         assert np.abs(got - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
+
+
+@pytest.mark.parametrize("Lsz", [5, 9, 28])
+def test_anderson_stencil_matches_csr_kernel_and_oracle(lib_built, Lsz):
+    """Matrix-free Anderson stencil: same terms in the same order as the CSR kernel."""
+    import sparse_matrix_algorithms_b200 as S
+
+    A = M.anderson3d(Lsz, 16.5, 3)
+    st = S.AndersonOperator(Lsz, 16.5, 3)
+    csr = S.SparseOperator(A)
+    smin, smax = _bounds(A)
+    for b, K in [(1, 7), (8, 60), (32, 130)]:
+        Q = M.splitmix_normal(b, A.shape[0], b)
+        c = O.build_coeffs(K, smin, smax, 0.0, -0.4, 0.4, "step", True)
+        y_st = S.apply_poly_block(st, Q, c, smin, smax)
+        y_csr = S.apply_poly_block(csr, Q, c, smin, smax)
+        scale = max(np.abs(y_csr).max(), 1.0)
+        assert np.abs(y_st - y_csr).max() <= 1e-15 * scale
+        ref = O.apply_poly_block(A, Q, c, smin, smax)
+        assert np.abs(y_st - ref).max() <= 1e-12 * max(np.abs(ref).max(), np.abs(Q).max())
+
+
+@pytest.mark.parametrize("Lc", [4, 10, 14, 18])
+def test_xxz_stencil_matches_oracle(lib_built, Lc):
+    import sparse_matrix_algorithms_b200 as S
+
+    A = M.xxz_sz0(Lc, 5.0, 1)
+    st = S.XXZOperator(Lc, 5.0, 1)
+    assert st.n == A.shape[0]
+    smin, smax = _bounds(A)
+    for b, K in [(2, 9), (16, 80)]:
+        Q = M.splitmix_normal(b + 1, A.shape[0], b)
+        c = O.build_coeffs(K, smin, smax, 0.0, -0.4, 0.4, "delta", True)
+        ref = O.apply_poly_block(A, Q, c, smin, smax)
+        got = S.apply_poly_block(st, Q, c, smin, smax)
+        assert np.abs(got - ref).max() <= 1e-12 * max(np.abs(ref).max(), np.abs(Q).max())
 
 
 def _device(arr):

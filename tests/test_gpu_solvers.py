@@ -239,3 +239,122 @@ def test_interval_outside_bounds_warns_then_raises(lib_built, capfd):
         S.chebyshev_poly_real_symm_sparse(M.lap1d(200), 1.0, 1.2, smin=1.1, smax=4.0, m0=8,
                                           degree=10, maxiter=1)
     assert "not contained" in capfd.readouterr().err
+
+
+def test_polfed_and_chebyshev_on_xxz_stencil_operator(lib_built):
+    """Both solvers on the matrix-free XXZ stencil (no stored matrix) against the dense
+    spectrum; bounds from GPU Lanczos on the stencil itself."""
+    import sparse_matrix_algorithms_b200 as S
+
+    A = M.xxz_sz0(12, 5.0, 1)
+    lam_all = np.linalg.eigvalsh(A.toarray())
+    nrm = _norm2(lam_all)
+    mid = int(np.argmin(np.abs(lam_all - 0.5 * (lam_all[0] + lam_all[-1]))))
+    emin, emax = _window_with_gaps(lam_all, mid - 10, mid + 9)
+    op = S.XXZOperator(12, 5.0, 1)
+    smin, smax = S.lanczos_bounds(op, steps=60)
+    assert smin <= lam_all[0] and smax >= lam_all[-1]
+    lam, X, res = S.polfed(op, 20, 800, s=8, smin=smin, smax=smax, sigma=0.5 * (emin + emax),
+                           emin=emin, emax=emax, mmax=10)
+    assert lam.size == 20
+    assert np.abs(np.sort(lam) - lam_all[mid - 10:mid + 10]).max() < 1e-12 * nrm
+    assert res.max() < 1e-10 * nrm
+    lam2, X2, res2 = S.chebyshev_poly_real_symm_sparse(op, emin, emax, smin=smin, smax=smax,
+                                                       m0=40, degree=800, maxiter=10,
+                                                       window_type="step")
+    assert lam2.size == 20
+    assert np.abs(lam2 - lam_all[mid - 10:mid + 10]).max() < 1e-12 * nrm
+
+
+# ---------------------------------------------------------------------- bounds
+@pytest.mark.parametrize("name", ["anderson_L20", "xxz_L18"])
+def test_lanczos_bounds_enclose_spectrum_and_beat_gershgorin(lib_built, name):
+    import sparse_matrix_algorithms_b200 as S
+    from conftest import GOLDEN
+
+    g = np.load(f"{GOLDEN}/{name}_spectrum.npz")
+    lo_true, hi_true = float(g["lam_min"]), float(g["lam_max"])
+    A = M.config_matrix(name)
+    lo, hi = S.lanczos_bounds(A, steps=80)
+    glo, ghi = O.gershgorin_bounds(A)
+    assert lo <= lo_true and hi >= hi_true  # encloses the spectrum
+    assert glo <= lo and hi <= ghi  # never looser than Gershgorin
+    assert (hi - lo) < 0.95 * (ghi - glo)
+    assert (hi - lo) < 1.01 * (hi_true - lo_true)
+
+
+def test_lanczos_bounds_stencil_operator(lib_built):
+    import sparse_matrix_algorithms_b200 as S
+
+    lo, hi = S.lanczos_bounds(S.Lap1dOperator(3000), steps=120)
+    ex = M.lap1d_exact_eigs(3000)
+    assert lo <= ex[0] and hi >= ex[-1] and hi - lo < 4.01
+
+
+# ---------------------------------------------------------------------- locking, precision
+def _c1_reference():
+    from conftest import GOLDEN
+
+    g = np.load(f"{GOLDEN}/anderson_L20_spectrum.npz")
+    c = g["central"]
+    exact = c[(c >= -0.05) & (c <= 0.05)]
+    return exact, max(abs(float(g["lam_min"])), abs(float(g["lam_max"])))
+
+
+def test_chebyshev_locking_c1(lib_built):
+    """Locking (lock=True): same eigenpairs as without, fewer filtered columns."""
+    import sparse_matrix_algorithms_b200 as S
+
+    exact, nrm = _c1_reference()
+    A = S.SparseOperator(M.config_matrix("anderson_L20"))
+    kw = dict(m0=64, degree=1500, maxiter=12, window_type="delta", sigma=0.0, tol=1e-11)
+    st0, st1 = {}, {}
+    lam0, X0, res0 = S.chebyshev_poly_real_symm_sparse(None, A.n, -0.05, 0.05, matblock=A,
+                                                       smin=-14.25, smax=14.25, stats=st0, **kw)
+    lam1, X1, res1 = S.chebyshev_poly_real_symm_sparse(None, A.n, -0.05, 0.05, matblock=A,
+                                                       smin=-14.25, smax=14.25, lock=True,
+                                                       stats=st1, **kw)
+    for lam, res in [(lam0, res0), (lam1, res1)]:
+        assert lam.size == exact.size
+        assert np.abs(lam - exact).max() <= 1e-12 * nrm
+        assert res.max() <= 1e-10 * nrm
+    assert st1["locked"] > 0
+    assert st1["spmm_columns"] < st0["spmm_columns"]
+    Ad = M.config_matrix("anderson_L20")
+    assert np.abs(np.linalg.norm(Ad @ X1 - X1 * lam1, axis=0) - res1).max() < 1e-12
+    assert np.abs(X1.T @ X1 - np.eye(lam1.size)).max() < 1e-10
+
+
+def test_chebyshev_mixed_precision_c1(lib_built):
+    """MIXED: FP32 filter first, FP64 for the final iterations; FP64-quality pairs."""
+    import sparse_matrix_algorithms_b200 as S
+
+    exact, nrm = _c1_reference()
+    A = S.SparseOperator(M.config_matrix("anderson_L20"))
+    st = {}
+    lam, X, res = S.chebyshev_poly_real_symm_sparse(
+        None, A.n, -0.05, 0.05, matblock=A, smin=-14.25, smax=14.25, m0=64, degree=1500,
+        maxiter=16, window_type="delta", sigma=0.0, precision="mixed", stats=st)
+    assert st["fp32_filter_calls"] >= 1
+    assert lam.size == exact.size
+    assert np.abs(lam - exact).max() <= 1e-12 * nrm
+    assert res.max() <= 1e-10 * nrm
+
+
+def test_polfed_mixed_precision_xxz(lib_built):
+    """POLFED with an FP32-filtered basis and FP64 polishing."""
+    import sparse_matrix_algorithms_b200 as S
+
+    A = M.xxz_sz0(12, 5.0, 1)
+    lam_all = np.linalg.eigvalsh(A.toarray())
+    nrm = _norm2(lam_all)
+    mid = int(np.argmin(np.abs(lam_all - 0.5 * (lam_all[0] + lam_all[-1]))))
+    emin, emax = _window_with_gaps(lam_all, mid - 10, mid + 9)
+    smin, smax = O.gershgorin_bounds(A)
+    st = {}
+    lam, X, res = S.polfed(A, 20, 800, s=8, smin=smin, smax=smax, sigma=0.5 * (emin + emax),
+                           emin=emin, emax=emax, mmax=10, precision="mixed", stats=st)
+    assert st["fp32_filter_calls"] >= 1
+    assert lam.size == 20
+    assert np.abs(np.sort(lam) - lam_all[mid - 10:mid + 10]).max() <= 1e-12 * nrm
+    assert res.max() <= 1e-10 * nrm

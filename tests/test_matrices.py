@@ -82,6 +82,23 @@ def test_xxz_sizes_and_density():
     assert abs(A.nnz / A.shape[0] - (1 + L * L / (2 * (L - 1)))) < 1e-9
 
 
+def test_matrix_market_round_trip_exact(tmp_path):
+    for A in [M.xxz_sz0(8, 3.0, 2), M.anderson3d(4, 16.5, 1)]:
+        p = os.path.join(tmp_path, "a.mtx")
+        M.save_mtx(p, A, comment="test matrix")
+        head = open(p).readline()
+        assert head.strip() == "%%MatrixMarket matrix coordinate real symmetric"
+        B = M.load_mtx(p)
+        for arr in ("indptr", "indices", "data"):  # every double recovered exactly
+            assert np.array_equal(getattr(A, arr), getattr(B, arr))
+    G = M._canonical(sp.csr_matrix(np.array([[1.0, 2.0], [0.0, 3.0]])))
+    p = os.path.join(tmp_path, "g.mtx")
+    M.save_mtx(p, G)
+    H = M.load_mtx(p)
+    assert "general" in open(p).readline()
+    assert np.array_equal(H.toarray(), G.toarray())
+
+
 def test_csr_file_round_trip(tmp_path):
     A = M.anderson3d(5, 16.5, 2)
     p = os.path.join(tmp_path, "a.csr")
