@@ -135,8 +135,28 @@ typedef struct sma_stats {
   int64_t fp32_filter_calls; /* filter applications run in FP32 (FP32 / MIXED precision) */
   int64_t locked;         /* pairs locked during the solve (Chebyshev with lock = 1) */
   int64_t polish_iterations; /* FP64 polishing iterations after an FP32 POLFED basis */
-  int64_t reserved[4];
+  int64_t graph_replays;  /* CUDA graph launches of the batched slicing filter */
+  int64_t reserved[3];
 } sma_stats;
+
+/* Options of batched spectrum slicing (sma_slice_solve); every window runs Chebyshev
+ * subspace iteration with the matrix-free overload's termination rule
+ * (chebyshev_subspace_iteration.jl:827-836). */
+typedef struct sma_slice_opts {
+  double smin, smax;       /* spectral bounds, used when has_bounds != 0 (else Gershgorin) */
+  int64_t has_bounds;
+  int64_t maxiter;         /* iterations per window, at most */
+  double tol;              /* absolute residual below which a window has converged */
+  double res_gate;         /* residual gate of the convergence count */
+  int64_t jackson;
+  int64_t two_hit;         /* 1: a window stops after two consecutive converged iterations */
+  int64_t seed;            /* window w starts from the random block of seed + w */
+  int64_t window_type;     /* sma_window; delta windows centre on (emin + emax) / 2 */
+  int64_t precision;       /* sma_precision; MIXED switches each window separately */
+  int64_t graph;           /* 1: record the batched filter into a CUDA graph and replay it */
+  int64_t debug;           /* 1: one progress line per window and iteration on stdout */
+  int64_t reserved[8];
+} sma_slice_opts;
 
 /* ---------------------------------------------------------------- library, context */
 int sma_abi_version(void);
@@ -239,6 +259,20 @@ int sma_cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts *op
 int sma_polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polfed_opts *opts,
                      sma_result **out);
 
+/* Batched spectrum slicing (no counterpart in the reference, which solves one window per
+ * call): nwin windows [emin[w], emax[w]] over the same operator, each with its own filter
+ * degree[w] and subspace width m0[w] (rounded up to a multiple of 8), solved together.
+ * Every filter application runs ONE batched Clenshaw recurrence over the concatenation
+ * of the windows' blocks: windows sorted by degree, each with its own coefficients, a
+ * window's columns joining the recurrence at its own degree, so each window's filtered
+ * block is bit-identical to a single-window filter.  Converged windows leave the batch.
+ * Explicit sparse matrices only.  The result holds the pairs of window 0, then window 1,
+ * ..., each by eigenvalue; sma_result_windows gives the window of every pair. */
+void sma_slice_opts_default(sma_slice_opts *o);
+int sma_slice_solve(sma_op *op, int64_t nwin, const double *emin, const double *emax,
+                    const int64_t *degree, const int64_t *m0, const sma_slice_opts *opts,
+                    sma_result **out);
+
 /* ---------------------------------------------------------------- results */
 /* k = number of returned pairs, n = vector length. */
 int sma_result_count(const sma_result *r, int64_t *k, int64_t *n);
@@ -246,6 +280,8 @@ int sma_result_count(const sma_result *r, int64_t *k, int64_t *n);
  * the three pointers may be NULL. */
 int sma_result_copy(const sma_result *r, double *lam, double *X, double *res);
 int sma_result_stats(const sma_result *r, sma_stats *stats);
+/* Window index of each returned pair (k int64 values; 0 for single-window solvers). */
+int sma_result_windows(const sma_result *r, int64_t *win);
 int sma_result_free(sma_result *r);
 
 #ifdef __cplusplus

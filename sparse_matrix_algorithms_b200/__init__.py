@@ -27,5 +27,6 @@ from .api import (  # noqa: F401
     jackson_kernel,
     lanczos_bounds,
     polfed,
+    slice_spectrum,
 )
 from . import matrices  # noqa: F401

@@ -73,13 +73,22 @@ class PolfedOpts(ctypes.Structure):
                 ("reserved", c_int64 * 8)]
 
 
+class SliceOpts(ctypes.Structure):
+    _fields_ = [("smin", c_double), ("smax", c_double), ("has_bounds", c_int64),
+                ("maxiter", c_int64), ("tol", c_double), ("res_gate", c_double),
+                ("jackson", c_int64), ("two_hit", c_int64), ("seed", c_int64),
+                ("window_type", c_int64), ("precision", c_int64), ("graph", c_int64),
+                ("debug", c_int64), ("reserved", c_int64 * 8)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("iterations", c_int64), ("basis_dim", c_int64), ("spmm_steps", c_int64),
                 ("spmm_columns", c_int64), ("filter_ms", c_double), ("orth_ms", c_double),
                 ("rr_ms", c_double), ("total_ms", c_double), ("filter_bytes", c_double),
                 ("qr_fallbacks", c_int64), ("warnings", c_int64), ("kernel_launches", c_int64),
                 ("fp32_filter_calls", c_int64), ("locked", c_int64),
-                ("polish_iterations", c_int64), ("reserved", c_int64 * 4)]
+                ("polish_iterations", c_int64), ("graph_replays", c_int64),
+                ("reserved", c_int64 * 3)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
@@ -130,9 +139,13 @@ SIGNATURES = [
                                ctypes.POINTER(c_void_p)]),
     ("sma_polfed_solve", c_int, [c_void_p, c_int64, c_int64, ctypes.POINTER(PolfedOpts),
                                  ctypes.POINTER(c_void_p)]),
+    ("sma_slice_opts_default", None, [ctypes.POINTER(SliceOpts)]),
+    ("sma_slice_solve", c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
+                                ctypes.POINTER(SliceOpts), ctypes.POINTER(c_void_p)]),
     ("sma_result_count", c_int, [c_void_p, ctypes.POINTER(c_int64), ctypes.POINTER(c_int64)]),
     ("sma_result_copy", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("sma_result_stats", c_int, [c_void_p, ctypes.POINTER(Stats)]),
+    ("sma_result_windows", c_int, [c_void_p, c_void_p]),
     ("sma_result_free", c_int, [c_void_p]),
 ]
 

@@ -452,3 +452,48 @@ def polfed(A, *args, s: int = 8, smin=None, smax=None, sigma: float = 0.0,
     L.check(L.load().sma_polfed_solve(op.handle, int(nev), int(degree), ctypes.byref(o),
                                       ctypes.byref(h)))
     return _take_result(h, stats)
+
+
+# ====================================================================== batched slicing
+def slice_spectrum(A, windows, degrees, m0s, *, smin=None, smax=None, maxiter: int = 8,
+                   tol: float = 1e-10, res_gate: float = 1e-6, jackson: bool = True,
+                   two_hit: bool = True, seed: int = 1, window_type="step",
+                   precision: str = "fp64", graph: bool = True, debug: bool = False,
+                   stats: Optional[dict] = None):
+    """Batched spectrum slicing (an extension; the reference solves one window per call).
+
+    ``windows`` is a sequence of ``(emin, emax)``; window ``w`` runs Chebyshev subspace
+    iteration with degree ``degrees[w]`` and width ``m0s[w]`` (rounded up to a multiple
+    of 8), seed ``seed + w`` and the matrix-free overload's termination rule, and every
+    iteration filters all unconverged windows in ONE batched recurrence (graph-captured
+    when ``graph``).  Returns ``(lam, X, res, win)``: per window its pairs by eigenvalue,
+    windows in order, ``win[j]`` the window of pair ``j``.
+    """
+    op = A if isinstance(A, _DeviceOp) else _resolve_sparse(A)
+    w = np.asarray(windows, dtype=np.float64).reshape(-1, 2)
+    emin = np.ascontiguousarray(w[:, 0])
+    emax = np.ascontiguousarray(w[:, 1])
+    deg = np.ascontiguousarray(degrees, dtype=np.int64)
+    m0 = np.ascontiguousarray(m0s, dtype=np.int64)
+    if not (deg.size == m0.size == emin.size):
+        raise ArgumentError(L.SMA_ERR_ARG, "windows, degrees and m0s differ in length")
+    o = L.SliceOpts()
+    lib = L.load()
+    lib.sma_slice_opts_default(ctypes.byref(o))
+    if smin is not None and smax is not None:
+        o.smin, o.smax, o.has_bounds = float(smin), float(smax), 1
+    o.maxiter, o.tol, o.res_gate = int(maxiter), float(tol), float(res_gate)
+    o.jackson, o.two_hit, o.seed = int(jackson), int(two_hit), int(seed)
+    o.window_type, o.precision = _window(window_type), L.PRECISIONS[precision]
+    o.graph, o.debug = int(graph), int(debug)
+    h = ctypes.c_void_p()
+    L.check(lib.sma_slice_solve(op.handle, int(emin.size), emin.ctypes.data, emax.ctypes.data,
+                                deg.ctypes.data, m0.ctypes.data, ctypes.byref(o),
+                                ctypes.byref(h)))
+    k = ctypes.c_int64()
+    L.check(lib.sma_result_count(h, ctypes.byref(k), None))
+    win = np.zeros(k.value, dtype=np.int64)
+    if k.value:
+        L.check(lib.sma_result_windows(h, win.ctypes.data))
+    lam, X, res = _take_result(h, stats)
+    return lam, X, res, win

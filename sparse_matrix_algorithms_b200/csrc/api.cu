@@ -11,6 +11,8 @@
 namespace sma {
 sma_result *cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts &o);
 sma_result *polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polfed_opts &o);
+sma_result *slice_solve(sma_op *op, int64_t nwin, const double *emin, const double *emax,
+                        const int64_t *degree, const int64_t *m0, const sma_slice_opts &o);
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string &msg) { g_last_error = msg; }
@@ -456,6 +458,37 @@ int sma_polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polfed_o
   });
 }
 
+void sma_slice_opts_default(sma_slice_opts *o) {
+  if (!o) return;
+  *o = sma_slice_opts{};
+  o->has_bounds = 0;
+  o->maxiter = 8;
+  o->tol = 1e-10;
+  o->res_gate = 1e-6;
+  o->jackson = 1;
+  o->two_hit = 1;
+  o->seed = 1;
+  o->window_type = SMA_WINDOW_STEP;
+  o->precision = SMA_PREC_FP64;
+  o->graph = 1;
+  o->debug = 0;
+}
+
+int sma_slice_solve(sma_op *op, int64_t nwin, const double *emin, const double *emax,
+                    const int64_t *degree, const int64_t *m0, const sma_slice_opts *opts,
+                    sma_result **out) {
+  return guarded([&] {
+    check_op(op);
+    require(out != nullptr, SMA_ERR_ARG, "null output pointer");
+    *out = nullptr;
+    sma_slice_opts o;
+    if (opts) o = *opts; else sma_slice_opts_default(&o);
+    if (o.has_bounds) check_bounds(o.smin, o.smax);
+    DeviceGuard g(op->ctx->device);
+    *out = slice_solve(op, nwin, emin, emax, degree, m0, o);
+  });
+}
+
 int sma_result_count(const sma_result *r, int64_t *k, int64_t *n) {
   return guarded([&] {
     require(r != nullptr, SMA_ERR_ARG, "null result");
@@ -484,6 +517,13 @@ int sma_result_stats(const sma_result *r, sma_stats *stats) {
   return guarded([&] {
     require(r != nullptr && stats != nullptr, SMA_ERR_ARG, "null argument");
     *stats = r->stats;
+  });
+}
+
+int sma_result_windows(const sma_result *r, int64_t *win) {
+  return guarded([&] {
+    require(r != nullptr && win != nullptr, SMA_ERR_ARG, "null argument");
+    for (int64_t j = 0; j < r->k; ++j) win[j] = r->win.empty() ? 0 : r->win[j];
   });
 }
 

@@ -76,12 +76,13 @@ __device__ __forceinline__ void row_product(const int *__restrict__ cols, const 
   }
 }
 
-template <typename T, int V, int G, int U, bool HQ, bool HS, bool HB>
+template <typename T, int V, int G, int U, bool HQ, bool HS, bool HB, bool PC>
 __global__ void __launch_bounds__(kThreads)
 direct_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
               const T *__restrict__ val, int64_t n, int b, const T *__restrict__ Q, int64_t ldq,
               const T *__restrict__ B1, const T *__restrict__ B2, int64_t ldb,
-              T *__restrict__ out, int64_t ldo, T ck, T alpha, T beta) {
+              T *__restrict__ out, int64_t ldo, T ck, T alpha, T beta,
+              const T *__restrict__ cseg, const int *__restrict__ colseg8) {
   constexpr int kRows = kThreads / G;
   const int64_t row = (int64_t)blockIdx.x * kRows + threadIdx.x / G;
   if (row >= n) return;
@@ -96,16 +97,19 @@ direct_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
     if constexpr (HS) ldv<T, V>(B1 + row * ldb + c0, s);
     if constexpr (HB) ldv<T, V>(B2 + row * ldb + c0, t);
     row_product<T, V, U>(colind, val, 0, start, end, B1 + c0, ldb, acc);
-    epilogue<T, V, HQ, HS, HB>(out + row * ldo + c0, acc, q, s, t, ck, alpha, beta);
+    T ckc = ck;
+    if constexpr (PC) ckc = __ldg(cseg + __ldg(colseg8 + (c0 >> 3)));
+    epilogue<T, V, HQ, HS, HB>(out + row * ldo + c0, acc, q, s, t, ckc, alpha, beta);
   }
 }
 
-template <typename T, int V, int G, int U, bool HQ, bool HS, bool HB>
+template <typename T, int V, int G, int U, bool HQ, bool HS, bool HB, bool PC>
 __global__ void __launch_bounds__(kThreads)
 staged_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
               const T *__restrict__ val, int64_t n, int b, const T *__restrict__ Q, int64_t ldq,
               const T *__restrict__ B1, const T *__restrict__ B2, int64_t ldb,
-              T *__restrict__ out, int64_t ldo, T ck, T alpha, T beta) {
+              T *__restrict__ out, int64_t ldo, T ck, T alpha, T beta,
+              const T *__restrict__ cseg, const int *__restrict__ colseg8) {
   constexpr int kRows = kThreads / G;
   __shared__ int s_col[kStage];
   __shared__ T s_val[kStage];
@@ -135,7 +139,9 @@ staged_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
     if constexpr (HB) ldv<T, V>(B2 + row * ldb + c0, t);
     if (staged) row_product<T, V, U>(s_col, s_val, base, start, end, B1 + c0, ldb, acc);
     else row_product<T, V, U>(colind, val, 0, start, end, B1 + c0, ldb, acc);
-    epilogue<T, V, HQ, HS, HB>(out + row * ldo + c0, acc, q, s, t, ck, alpha, beta);
+    T ckc = ck;
+    if constexpr (PC) ckc = __ldg(cseg + __ldg(colseg8 + (c0 >> 3)));
+    epilogue<T, V, HQ, HS, HB>(out + row * ldo + c0, acc, q, s, t, ckc, alpha, beta);
   }
 }
 
@@ -223,6 +229,10 @@ struct Args {
   T *out;
   int64_t ldo;
   double ck, alpha, beta;
+  // batched spectrum slicing: per-segment coefficients of this step (cseg[segment]) and the
+  // segment of every 8 consecutive columns (colseg8[column / 8]); null for one segment
+  const T *cseg = nullptr;
+  const int *colseg8 = nullptr;
 };
 
 template <typename T, int V, int G, int U, bool HQ, bool HS, bool HB>
@@ -232,19 +242,35 @@ void launch_one(int fam, const Args<T> &a) {
   else val = (const T *)a.op->val32;
   constexpr int kRows = kThreads / G;
   const unsigned grid = (unsigned)((a.op->n + kRows - 1) / kRows);
+  if constexpr (HQ && HS && HB) {
+    if (a.cseg) {
+      if (fam == 0)
+        direct_kernel<T, V, G, U, true, true, true, true><<<grid, kThreads, 0, a.st>>>(
+            a.op->rowptr, a.op->colind, val, a.op->n, (int)a.b, a.Q, a.ldq, a.B1, a.B2, a.ldb,
+            a.out, a.ldo, T(0), (T)a.alpha, (T)a.beta, a.cseg, a.colseg8);
+      else
+        staged_kernel<T, V, G, U, true, true, true, true><<<grid, kThreads, 0, a.st>>>(
+            a.op->rowptr, a.op->colind, val, a.op->n, (int)a.b, a.Q, a.ldq, a.B1, a.B2, a.ldb,
+            a.out, a.ldo, T(0), (T)a.alpha, (T)a.beta, a.cseg, a.colseg8);
+      SMA_CHECK_LAUNCH();
+      return;
+    }
+  }
+  if (a.cseg) throw Error(SMA_ERR_INTERNAL, "segmented Clenshaw step needs the full variant");
   if (fam == 0)
-    direct_kernel<T, V, G, U, HQ, HS, HB><<<grid, kThreads, 0, a.st>>>(
+    direct_kernel<T, V, G, U, HQ, HS, HB, false><<<grid, kThreads, 0, a.st>>>(
         a.op->rowptr, a.op->colind, val, a.op->n, (int)a.b, a.Q, a.ldq, a.B1, a.B2, a.ldb, a.out,
-        a.ldo, (T)a.ck, (T)a.alpha, (T)a.beta);
+        a.ldo, (T)a.ck, (T)a.alpha, (T)a.beta, nullptr, nullptr);
   else
-    staged_kernel<T, V, G, U, HQ, HS, HB><<<grid, kThreads, 0, a.st>>>(
+    staged_kernel<T, V, G, U, HQ, HS, HB, false><<<grid, kThreads, 0, a.st>>>(
         a.op->rowptr, a.op->colind, val, a.op->n, (int)a.b, a.Q, a.ldq, a.B1, a.B2, a.ldb, a.out,
-        a.ldo, (T)a.ck, (T)a.alpha, (T)a.beta);
+        a.ldo, (T)a.ck, (T)a.alpha, (T)a.beta, nullptr, nullptr);
   SMA_CHECK_LAUNCH();
 }
 
 template <typename T, int G, int NB, bool HQ, bool HS, bool HB>
 void launch_async(const Args<T> &a) {
+  if (a.cseg) throw Error(SMA_ERR_INTERNAL, "the asynchronous family has no segmented variant");
   const T *val;
   if constexpr (sizeof(T) == 8) val = (const T *)a.op->val64;
   else val = (const T *)a.op->val32;
@@ -326,7 +352,8 @@ void step(const Args<T> &a) {
     if (v * (int)sizeof(T) <= 32 && ok(v)) vmax = v;
   const uint64_t key = ((uint64_t)sizeof(T) << 56) | ((uint64_t)vmax << 52) |
                        ((uint64_t)((HQ ? 4 : 0) | (HS ? 2 : 0) | (HB ? 1 : 0)) << 48) |
-                       ((uint64_t)a.b << 24) | (uint64_t)std::min<int64_t>(a.ldb, 0xFFFFFF);
+                       (a.cseg ? (1ull << 51) : 0ull) | ((uint64_t)a.b << 24) |
+                       (uint64_t)std::min<int64_t>(a.ldb, 0xFFFFFF);
   CsrTune &tu = const_cast<sma_op *>(op)->tuned[key];
   if (tu.chosen >= 0) return launch_cfg<T, HQ, HS, HB>(tu.chosen, a);
   if (tu.cands.empty()) {
@@ -341,7 +368,7 @@ void step(const Args<T> &a) {
           tu.cands.push_back(enc(fam, V, G, 4));
         }
       }
-    if (vmax * (int)sizeof(T) >= 16) {  // the ASYNC family moves 16-byte chunks
+    if (vmax * (int)sizeof(T) >= 16 && !a.cseg) {  // the ASYNC family moves 16-byte chunks
       const int V = 16 / (int)sizeof(T);
       const int64_t lanes = (a.b + V - 1) / V;
       const int g0 = lanes <= 4 ? 4 : lanes <= 8 ? 8 : lanes <= 16 ? 16 : 32;
@@ -431,7 +458,8 @@ void step_untuned(const Args<T> &a) {
     if (v * (int)sizeof(T) <= 32 && ok(v)) vmax = v;
   const uint64_t key = ((uint64_t)sizeof(T) << 56) | ((uint64_t)vmax << 52) |
                        ((uint64_t)((HQ ? 4 : 0) | (HS ? 2 : 0) | (HB ? 1 : 0)) << 48) |
-                       ((uint64_t)a.b << 24) | (uint64_t)std::min<int64_t>(a.ldb, 0xFFFFFF);
+                       (a.cseg ? (1ull << 51) : 0ull) | ((uint64_t)a.b << 24) |
+                       (uint64_t)std::min<int64_t>(a.ldb, 0xFFFFFF);
   const auto it = a.op->tuned.find(key);
   if (it != a.op->tuned.end() && it->second.chosen >= 0)
     return launch_cfg<T, HQ, HS, HB>(it->second.chosen, a);
@@ -450,5 +478,21 @@ void csr_clenshaw_step_untuned(const sma_op *op, cudaStream_t st, int64_t b, con
   if (Q && has_self && B2) return csr::step_untuned<T, true, true, true>(a);
   if (Q && has_self && !B2) return csr::step_untuned<T, true, true, false>(a);
   throw Error(SMA_ERR_INTERNAL, "unsupported Clenshaw step variant");
+}
+
+// The segmented step of batched spectrum slicing: column c takes the coefficient
+// cseg[colseg8[c / 8]]; Q, B1 and B2 are all read.  tuned = false uses the operator's
+// cached configuration (or the default one) and creates no events, so that it may be
+// recorded into a CUDA graph.
+template <typename T>
+void csr_clenshaw_step_seg(const sma_op *op, cudaStream_t st, int64_t b, const T *Q, int64_t ldq,
+                           const T *B1, const T *B2, int64_t ldb, T *out, int64_t ldo,
+                           const T *cseg, const int *colseg8, double alpha, double beta,
+                           bool tuned) {
+  csr::Args<T> a{op, st, b, Q, ldq, B1, B2, ldb, out, ldo, 0.0, alpha, beta};
+  a.cseg = cseg;
+  a.colseg8 = colseg8;
+  if (tuned) return csr::step<T, true, true, true>(a);
+  csr::step_untuned<T, true, true, true>(a);
 }
 }  // namespace sma

@@ -180,6 +180,18 @@ template <typename T>
 void csr_clenshaw_step(const sma_op *op, cudaStream_t st, int64_t b, const T *Q, int64_t ldq,
                        const T *B1, const T *B2, int64_t ldb, T *out, int64_t ldo, double ck,
                        double alpha, double beta, bool has_self);
+// The CSR step without the autotuner (cached or default configuration, no events).
+template <typename T>
+void csr_clenshaw_step_untuned(const sma_op *op, cudaStream_t st, int64_t b, const T *Q,
+                               int64_t ldq, const T *B1, const T *B2, int64_t ldb, T *out,
+                               int64_t ldo, double ck, double alpha, double beta, bool has_self);
+// The segmented CSR step of batched slicing: column c uses the coefficient
+// cseg[colseg8[c / 8]] (csr_clenshaw.cuh).
+template <typename T>
+void csr_clenshaw_step_seg(const sma_op *op, cudaStream_t st, int64_t b, const T *Q, int64_t ldq,
+                           const T *B1, const T *B2, int64_t ldb, T *out, int64_t ldo,
+                           const T *cseg, const int *colseg8, double alpha, double beta,
+                           bool tuned);
 // out = ck * Q
 template <typename T>
 void launch_scale_block(cudaStream_t st, int64_t n, int64_t b, const T *Q, int64_t ldq, T *out,
@@ -297,6 +309,7 @@ struct sma_result {
   std::vector<double> lam, res;
   double *X_dev = nullptr;  // row-major n x k (ld k), owned
   int64_t ldx = 0;
+  std::vector<int64_t> win;  // window of each pair (batched slicing); empty means all 0
   sma_ctx *ctx = nullptr;
   sma_stats stats{};
 };
