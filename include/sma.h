@@ -205,6 +205,20 @@ int sma_gershgorin_bounds(sma_op *op, double *smin, double *smax);
  * (explicit matrices, model stencils).  An estimate.  Any operator kind. */
 int sma_lanczos_bounds(sma_op *op, int64_t steps, int64_t seed, double *smin, double *smax);
 
+/* Stochastic Chebyshev moments of the spectral density, the kernel polynomial method (an
+ * extension; the reference has no density-of-states estimate):
+ *   mu[k] = (1/(n R)) sum_r z_r^T T_k(A_hat) z_r,  k < M,  A_hat = (A - c I)/d,
+ * with c, d the centre and half-width of [smin, smax] and R Rademacher vectors z_r drawn
+ * from the seeded SplitMix64 stream (mu[0] = 1 exactly).  FP64, ceil(M/2) block products
+ * of width R.  per_vec (may be NULL) receives the M x R per-vector moments, row-major.
+ * Any operator kind.  Synchronous. */
+int sma_kpm_moments(sma_op *op, int64_t M, int64_t R, int64_t seed, double smin, double smax,
+                    double *mu, double *per_vec);
+/* Number of eigenvalues in [emin, emax] predicted by the moments of an n x n operator:
+ * n times the integral of the Jackson-damped (jackson != 0) Chebyshev density series. */
+int sma_kpm_count(const double *mu, int64_t M, int64_t n, double smin, double smax,
+                  double emin, double emax, int64_t jackson, double *count);
+
 /* ---------------------------------------------------------------- filter coefficients */
 /* jackson_kernel(K): g[0..K] (chebyshev_subspace_iteration.jl:376-387). */
 int sma_jackson_kernel(int64_t K, double *g);
@@ -273,6 +287,34 @@ int sma_slice_solve(sma_op *op, int64_t nwin, const double *emin, const double *
                     const int64_t *degree, const int64_t *m0, const sma_slice_opts *opts,
                     sma_result **out);
 
+/* ---------------------------------------------------------------- learned window planner */
+/* A three-layer perceptron (in -> hid -> hid -> out, relu) with BF16 weights, FP32
+ * biases and FP32 arithmetic, trained on the GPU by the library's own forward, backward
+ * and Adam kernels (an extension: the reference picks degree and subspace size by hand).
+ * It maps a window's KPM moments and mapped bounds to corrections of the plain rule's
+ * filter degree, subspace width and eigenvalue count.  Parameters are packed as
+ * W1 (hid x in, row-major), b1, W2 (hid x hid), b2, W3 (out x hid), b3: FP32 masters,
+ * count = hid*in + hid + hid*hid + hid + out*hid + out.  Rows of X are samples. */
+typedef struct sma_mlp sma_mlp;
+int sma_mlp_create(sma_ctx *ctx, int64_t in, int64_t hid, int64_t out, int64_t seed,
+                   sma_mlp **net);
+int sma_mlp_destroy(sma_mlp *net);
+int sma_mlp_num_params(const sma_mlp *net, int64_t *count);
+int sma_mlp_get_params(const sma_mlp *net, float *params);
+/* Loads FP32 masters (their BF16 copies are made on the device) and resets Adam. */
+int sma_mlp_set_params(sma_mlp *net, const float *params);
+/* Y (B x out) = network(X (B x in)), host arrays. */
+int sma_mlp_forward(sma_mlp *net, const float *X, int64_t B, float *Y);
+/* Loss (1/B) sum w (Y - T)^2 (w may be NULL: ones) and its gradient with respect to the
+ * packed parameters (grad may be NULL), for host arrays X (B x in), T and w (B x out). */
+int sma_mlp_grad(sma_mlp *net, const float *X, const float *T, const float *w, int64_t B,
+                 float *loss, float *grad);
+/* steps of minibatch Adam (lr, minibatch rows, L2 weight decay) over N host rows, all on
+ * the device; loss_hist (may be NULL) receives the minibatch loss before each step. */
+int sma_mlp_train(sma_mlp *net, const float *X, const float *T, const float *w, int64_t N,
+                  int64_t steps, double lr, int64_t minibatch, int64_t seed,
+                  double weight_decay, float *loss_hist);
+
 /* ---------------------------------------------------------------- results */
 /* k = number of returned pairs, n = vector length. */
 int sma_result_count(const sma_result *r, int64_t *k, int64_t *n);
@@ -282,6 +324,11 @@ int sma_result_copy(const sma_result *r, double *lam, double *X, double *res);
 int sma_result_stats(const sma_result *r, sma_stats *stats);
 /* Window index of each returned pair (k int64 values; 0 for single-window solvers). */
 int sma_result_windows(const sma_result *r, int64_t *win);
+/* Per window of a slicing result (nwin entries each, either pointer may be NULL): the
+ * iterations it ran and whether it met its convergence rule (1) or ran out (0).  A
+ * single-window solver's result reports one window. */
+int sma_result_window_info(const sma_result *r, int64_t nwin, int64_t *iterations,
+                           int64_t *converged);
 int sma_result_free(sma_result *r);
 
 #ifdef __cplusplus

@@ -593,3 +593,51 @@ def _progress_line(m, lam, res):
     r90 = rs[min(max(int(round(0.9 * rs.size)), 1), rs.size) - 1]
     r95 = rs[min(max(int(round(0.95 * rs.size)), 1), rs.size) - 1]
     print(f"m={m}  inside={lam.size}  r90={r90}  r95={r95}  maxres={rs[-1]}")
+
+
+# ======================================================================================
+# Kernel polynomial method (no reference counterpart: the library's density-of-states
+# extension).  Restated from the published method (Weisse, Wellein, Alvermann, Fehske,
+# Rev. Mod. Phys. 78, 275 (2006), sections II.B-II.C) with the plain three-term
+# recurrence -- not the doubling identities the GPU uses -- so the two checks differ in
+# arithmetic.
+# ======================================================================================
+def kpm_moments(A, M: int, R: int, seed: int, smin: float, smax: float,
+                per_vector: bool = False):
+    """mu_k = (1/(n R)) sum_r z_r^T T_k(A_hat) z_r, k < M, Rademacher z_r."""
+    from sparse_matrix_algorithms_b200.matrices import splitmix_rademacher
+
+    n = A.shape[0]
+    c = 0.5 * (smin + smax)
+    d = 0.5 * (smax - smin)
+    A = sp.csr_matrix(A)
+    Z = splitmix_rademacher(seed, n, R)
+    pv = np.empty((M, R))
+    T0 = Z.copy()
+    pv[0] = np.einsum("ij,ij->j", Z, T0)
+    if M > 1:
+        T1 = (A @ T0 - c * T0) / d
+        pv[1] = np.einsum("ij,ij->j", Z, T1)
+        for k in range(2, M):
+            T2 = 2.0 * (A @ T1 - c * T1) / d - T0
+            pv[k] = np.einsum("ij,ij->j", Z, T2)
+            T0, T1 = T1, T2
+    pv /= n
+    mu = pv.mean(axis=1)
+    return (mu, pv) if per_vector else mu
+
+
+def kpm_count(mu, n: int, smin: float, smax: float, emin: float, emax: float,
+              jackson: bool = True) -> float:
+    """n times the integral over [emin, emax] of the damped Chebyshev density series."""
+    M = len(mu)
+    c = 0.5 * (smin + smax)
+    d = 0.5 * (smax - smin)
+    a = min(1.0, max(-1.0, (emin - c) / d))
+    b = min(1.0, max(-1.0, (emax - c) / d))
+    ta, tb = math.acos(a), math.acos(b)
+    g = jackson_kernel(M - 1) if jackson else np.ones(M)
+    k = np.arange(1, M)
+    s = g[0] * mu[0] * (ta - tb) + np.sum(2.0 * g[1:] * np.asarray(mu[1:]) *
+                                          (np.sin(k * ta) - np.sin(k * tb)) / k)
+    return float(n * s / math.pi)

@@ -25,6 +25,8 @@ from .api import (  # noqa: F401
     context,
     gershgorin_bounds,
     jackson_kernel,
+    kpm_count,
+    kpm_moments,
     lanczos_bounds,
     polfed,
     slice_spectrum,

@@ -133,6 +133,10 @@ SIGNATURES = [
     ("sma_spmm_dev", c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_int64]),
     ("sma_apply_poly_block_noalloc", c_int, [c_void_p, c_void_p, c_int64, c_double, c_double,
                                              c_void_p, c_int64, c_void_p, c_int64, c_int64]),
+    ("sma_kpm_moments", c_int, [c_void_p, c_int64, c_int64, c_int64, c_double, c_double,
+                                c_void_p, c_void_p]),
+    ("sma_kpm_count", c_int, [c_void_p, c_int64, c_int64, c_double, c_double, c_double,
+                              c_double, c_int64, ctypes.POINTER(c_double)]),
     ("sma_cheb_opts_default", None, [ctypes.POINTER(ChebOpts)]),
     ("sma_polfed_opts_default", None, [ctypes.POINTER(PolfedOpts)]),
     ("sma_cheb_solve", c_int, [c_void_p, c_double, c_double, ctypes.POINTER(ChebOpts),
@@ -142,10 +146,22 @@ SIGNATURES = [
     ("sma_slice_opts_default", None, [ctypes.POINTER(SliceOpts)]),
     ("sma_slice_solve", c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
                                 ctypes.POINTER(SliceOpts), ctypes.POINTER(c_void_p)]),
+    ("sma_mlp_create", c_int, [c_void_p, c_int64, c_int64, c_int64, c_int64,
+                               ctypes.POINTER(c_void_p)]),
+    ("sma_mlp_destroy", c_int, [c_void_p]),
+    ("sma_mlp_num_params", c_int, [c_void_p, ctypes.POINTER(c_int64)]),
+    ("sma_mlp_get_params", c_int, [c_void_p, c_void_p]),
+    ("sma_mlp_set_params", c_int, [c_void_p, c_void_p]),
+    ("sma_mlp_forward", c_int, [c_void_p, c_void_p, c_int64, c_void_p]),
+    ("sma_mlp_grad", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
+                             ctypes.POINTER(ctypes.c_float), c_void_p]),
+    ("sma_mlp_train", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int64,
+                              c_double, c_int64, c_int64, c_double, c_void_p]),
     ("sma_result_count", c_int, [c_void_p, ctypes.POINTER(c_int64), ctypes.POINTER(c_int64)]),
     ("sma_result_copy", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("sma_result_stats", c_int, [c_void_p, ctypes.POINTER(Stats)]),
     ("sma_result_windows", c_int, [c_void_p, c_void_p]),
+    ("sma_result_window_info", c_int, [c_void_p, c_int64, c_void_p, c_void_p]),
     ("sma_result_free", c_int, [c_void_p]),
 ]
 

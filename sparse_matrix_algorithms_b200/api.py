@@ -495,5 +495,42 @@ def slice_spectrum(A, windows, degrees, m0s, *, smin=None, smax=None, maxiter: i
     win = np.zeros(k.value, dtype=np.int64)
     if k.value:
         L.check(lib.sma_result_windows(h, win.ctypes.data))
+    if stats is not None:
+        its = np.zeros(emin.size, dtype=np.int64)
+        conv = np.zeros(emin.size, dtype=np.int64)
+        L.check(lib.sma_result_window_info(h, int(emin.size), its.ctypes.data, conv.ctypes.data))
+        stats["window_iterations"] = its
+        stats["window_converged"] = conv.astype(bool)
     lam, X, res = _take_result(h, stats)
     return lam, X, res, win
+
+
+# ====================================================================== KPM density of states
+def kpm_moments(A, M: int = 256, R: int = 16, *, smin=None, smax=None, seed: int = 11,
+                per_vector: bool = False):
+    """Stochastic Chebyshev moments ``mu[0..M-1]`` of the spectral density of ``A`` on the
+    GPU (an extension: the reference has no density-of-states estimate).  ``R``
+    Rademacher vectors; ``[smin, smax]`` defaults to the Gershgorin bounds.  With
+    ``per_vector`` also returns the ``M x R`` per-vector moments."""
+    op = _op_of(A)
+    if smin is None or smax is None:
+        if not hasattr(op, "gershgorin_bounds"):
+            raise ArgumentError(L.SMA_ERR_ARG, "pass smin and smax for a matrix-free operator")
+        smin, smax = op.gershgorin_bounds()
+    mu = np.empty(int(M))
+    pv = np.empty((int(M), int(R))) if per_vector else None
+    L.check(L.load().sma_kpm_moments(op.handle, int(M), int(R), int(seed), float(smin),
+                                     float(smax), mu.ctypes.data,
+                                     pv.ctypes.data if pv is not None else None))
+    return (mu, pv) if per_vector else mu
+
+
+def kpm_count(mu, n: int, smin: float, smax: float, emin: float, emax: float,
+              jackson: bool = True) -> float:
+    """Eigenvalue count in ``[emin, emax]`` predicted by KPM moments of an n x n matrix."""
+    m = np.ascontiguousarray(mu, dtype=np.float64)
+    out = ctypes.c_double()
+    L.check(L.load().sma_kpm_count(m.ctypes.data, int(m.size), int(n), float(smin),
+                                   float(smax), float(emin), float(emax), int(jackson),
+                                   ctypes.byref(out)))
+    return out.value

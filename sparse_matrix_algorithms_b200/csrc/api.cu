@@ -383,6 +383,26 @@ int sma_spmm_dev(sma_op *op, const double *X_dev, int64_t ldx, double *Y_dev, in
   });
 }
 
+int sma_kpm_moments(sma_op *op, int64_t M, int64_t R, int64_t seed, double smin, double smax,
+                    double *mu, double *per_vec) {
+  return guarded([&] {
+    check_op(op);
+    require(mu != nullptr, SMA_ERR_ARG, "null moment array");
+    check_bounds(smin, smax);
+    require(op->n > 0, SMA_ERR_ARG, "empty operator");
+    DeviceGuard g(op->ctx->device);
+    kpm_moments(op, M, R, (uint64_t)seed, smin, smax, mu, per_vec);
+  });
+}
+
+int sma_kpm_count(const double *mu, int64_t M, int64_t n, double smin, double smax,
+                  double emin, double emax, int64_t jackson, double *count) {
+  return guarded([&] {
+    require(mu != nullptr && count != nullptr, SMA_ERR_ARG, "null argument");
+    *count = kpm_count(mu, M, n, smin, smax, emin, emax, jackson != 0);
+  });
+}
+
 void sma_cheb_opts_default(sma_cheb_opts *o) {
   if (!o) return;
   *o = sma_cheb_opts{};
@@ -489,6 +509,88 @@ int sma_slice_solve(sma_op *op, int64_t nwin, const double *emin, const double *
   });
 }
 
+int sma_mlp_create(sma_ctx *ctx, int64_t in, int64_t hid, int64_t out, int64_t seed,
+                   sma_mlp **net) {
+  return guarded([&] {
+    require(ctx != nullptr && net != nullptr, SMA_ERR_ARG, "null argument");
+    require(in >= 1 && hid >= 1 && out >= 1, SMA_ERR_ARG, "layer sizes must be positive");
+    *net = nullptr;
+    DeviceGuard g(ctx->device);
+    auto *p = new sma_mlp();
+    p->ctx = ctx;
+    try {
+      mlp_init(p, in, hid, out, (uint64_t)seed);
+    } catch (...) {
+      delete p;
+      throw;
+    }
+    *net = p;
+  });
+}
+
+int sma_mlp_destroy(sma_mlp *net) {
+  return guarded([&] {
+    if (!net) return;
+    DeviceGuard g(net->ctx->device);
+    cudaStreamSynchronize(net->ctx->stream);
+    delete net;
+  });
+}
+
+int sma_mlp_num_params(const sma_mlp *net, int64_t *count) {
+  return guarded([&] {
+    require(net != nullptr && count != nullptr, SMA_ERR_ARG, "null argument");
+    *count = net->nparam;
+  });
+}
+
+int sma_mlp_get_params(const sma_mlp *net, float *params) {
+  return guarded([&] {
+    require(net != nullptr && params != nullptr, SMA_ERR_ARG, "null argument");
+    DeviceGuard g(net->ctx->device);
+    mlp_get_params(net, params);
+  });
+}
+
+int sma_mlp_set_params(sma_mlp *net, const float *params) {
+  return guarded([&] {
+    require(net != nullptr && params != nullptr, SMA_ERR_ARG, "null argument");
+    DeviceGuard g(net->ctx->device);
+    mlp_set_params(net, params);
+  });
+}
+
+int sma_mlp_forward(sma_mlp *net, const float *X, int64_t B, float *Y) {
+  return guarded([&] {
+    require(net != nullptr && B >= 0, SMA_ERR_ARG, "bad argument");
+    if (B == 0) return;
+    require(X != nullptr && Y != nullptr, SMA_ERR_ARG, "null array");
+    DeviceGuard g(net->ctx->device);
+    mlp_forward(net, X, B, Y);
+  });
+}
+
+int sma_mlp_grad(sma_mlp *net, const float *X, const float *T, const float *w, int64_t B,
+                 float *loss, float *grad) {
+  return guarded([&] {
+    require(net != nullptr && X != nullptr && T != nullptr && B >= 1, SMA_ERR_ARG, "bad argument");
+    DeviceGuard g(net->ctx->device);
+    const float l = mlp_grad(net, X, T, w, B, grad);
+    if (loss) *loss = l;
+  });
+}
+
+int sma_mlp_train(sma_mlp *net, const float *X, const float *T, const float *w, int64_t N,
+                  int64_t steps, double lr, int64_t minibatch, int64_t seed,
+                  double weight_decay, float *loss_hist) {
+  return guarded([&] {
+    require(net != nullptr && X != nullptr && T != nullptr, SMA_ERR_ARG, "null argument");
+    require(lr > 0.0, SMA_ERR_ARG, "learning rate must be positive");
+    DeviceGuard g(net->ctx->device);
+    mlp_train(net, X, T, w, N, steps, lr, minibatch, (uint64_t)seed, weight_decay, loss_hist);
+  });
+}
+
 int sma_result_count(const sma_result *r, int64_t *k, int64_t *n) {
   return guarded([&] {
     require(r != nullptr, SMA_ERR_ARG, "null result");
@@ -524,6 +626,19 @@ int sma_result_windows(const sma_result *r, int64_t *win) {
   return guarded([&] {
     require(r != nullptr && win != nullptr, SMA_ERR_ARG, "null argument");
     for (int64_t j = 0; j < r->k; ++j) win[j] = r->win.empty() ? 0 : r->win[j];
+  });
+}
+
+int sma_result_window_info(const sma_result *r, int64_t nwin, int64_t *iterations,
+                           int64_t *converged) {
+  return guarded([&] {
+    require(r != nullptr, SMA_ERR_ARG, "null result");
+    const int64_t have = r->win_iters.empty() ? 1 : (int64_t)r->win_iters.size();
+    require(nwin == have, SMA_ERR_ARG, "the result holds " + std::to_string(have) + " windows");
+    for (int64_t w = 0; w < nwin; ++w) {
+      if (iterations) iterations[w] = r->win_iters.empty() ? r->stats.iterations : r->win_iters[w];
+      if (converged) converged[w] = r->win_done.empty() ? 0 : r->win_done[w];
+    }
   });
 }
 

@@ -386,7 +386,11 @@ sma_result *slice_solve(sma_op *op, int64_t nwin, const double *emin, const doub
     }
   }
   int64_t wsum = 0;
-  for (Window &x : win) wsum += x.m0;
+  for (Window &x : win) {
+    wsum += x.m0;
+    r->win_iters.push_back(x.iterations);
+    r->win_done.push_back(x.done ? 1 : 0);
+  }
   stats.iterations = itmax;
   stats.basis_dim = wsum;
   stats.spmm_steps = total.steps;

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cublas_v2.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
 
@@ -243,6 +244,12 @@ void launch_add_diagonal(cudaStream_t st, int64_t k, double *G, int64_t ld, doub
 // Zero the strict lower triangle of a k x k column-major matrix
 void launch_zero_lower(cudaStream_t st, int64_t k, double *G, int64_t ld);
 
+// ------------------------------------------------------------------ KPM (kpm.cu)
+void kpm_moments(const sma_op *op, int64_t M, int64_t R, uint64_t seed, double smin,
+                 double smax, double *mu, double *per_vec);
+double kpm_count(const double *mu, int64_t M, int64_t n, double smin, double smax, double emin,
+                 double emax, bool jackson);
+
 // ------------------------------------------------------------------ host coefficient builders
 std::vector<double> jackson_kernel(int64_t K);
 std::vector<double> cheb_delta_coeffs(double sh, int64_t K, bool jackson);
@@ -310,6 +317,49 @@ struct sma_result {
   double *X_dev = nullptr;  // row-major n x k (ld k), owned
   int64_t ldx = 0;
   std::vector<int64_t> win;  // window of each pair (batched slicing); empty means all 0
+  std::vector<int64_t> win_iters, win_done;  // per window: iterations run, converged flag
   sma_ctx *ctx = nullptr;
   sma_stats stats{};
 };
+
+// ------------------------------------------------------------------ learned window planner (mlp.cu)
+// A three-layer perceptron with BF16 weights (FP32 masters) and its training state.
+struct sma_mlp {
+  sma_ctx *ctx = nullptr;
+  int64_t in = 0, hid = 0, out = 0;
+  int64_t nparam = 0;
+  // offsets into the packed parameter vector: W1 (hid x in), b1, W2 (hid x hid), b2,
+  // W3 (out x hid), b3
+  int64_t oW1 = 0, ob1 = 0, oW2 = 0, ob2 = 0, oW3 = 0, ob3 = 0;
+  sma::DevBuf<float> master, grad, m, v;
+  sma::DevBuf<__nv_bfloat16> wbf;
+  int64_t adam_t = 0;
+  // activations for the current batch
+  int64_t bcap = 0;
+  sma::DevBuf<float> h1, h2, y, d2, d1, dy, partial, loss;
+  void ensure(int64_t B) {
+    if (B <= bcap) return;
+    cudaStream_t st = ctx->stream;
+    bcap = B;
+    h1.alloc(B * hid, st);
+    h2.alloc(B * hid, st);
+    y.alloc(B * out, st);
+    d2.alloc(B * hid, st);
+    d1.alloc(B * hid, st);
+    dy.alloc(B * out, st);
+    partial.alloc(B, st);
+    loss.alloc(1, st);
+  }
+};
+
+namespace sma {
+void mlp_init(sma_mlp *net, int64_t in, int64_t hid, int64_t out, uint64_t seed);
+void mlp_set_params(sma_mlp *net, const float *p);
+void mlp_get_params(const sma_mlp *net, float *p);
+void mlp_forward(sma_mlp *net, const float *X_host, int64_t B, float *Y_host);
+float mlp_grad(sma_mlp *net, const float *X_host, const float *T_host, const float *w_host,
+               int64_t B, float *grad_host);
+void mlp_train(sma_mlp *net, const float *X_host, const float *T_host, const float *w_host,
+               int64_t N, int64_t steps, double lr, int64_t mb, uint64_t seed, double weight_decay,
+               float *loss_hist);
+}  // namespace sma

@@ -53,6 +53,18 @@ def splitmix_uniform(seed: int, count: int, offset: int = 0) -> np.ndarray:
     return (x >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
 
 
+def splitmix_rademacher(seed: int, n: int, m: int) -> np.ndarray:
+    """+-1 n x m block (column-major draw order): element (i, j), flat index k = i + j*n,
+    is -1 when the top bit of draw k of stream ``seed ^ 0x2545F4914F6CDD1D`` is set.  The
+    CUDA library's KPM start block uses the same rule."""
+    s = np.uint64((seed ^ 0x2545F4914F6CDD1D) & 0xFFFFFFFFFFFFFFFF)
+    k = np.arange(1, n * m + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        x = mix64(s + k * GOLDEN)
+    z = np.where((x >> np.uint64(63)) != 0, -1.0, 1.0)
+    return z.reshape((m, n)).T.copy(order="F")
+
+
 def splitmix_normal(seed: int, n: int, m: int) -> np.ndarray:
     """Standard normal n x m block (column-major draw order, like ``randn(n, m)``).
 

@@ -1,0 +1,327 @@
+"""Window planning for batched spectrum slicing: the plain rule and the learned planner.
+
+For every window [emin, emax] the slicing solver needs an eigenvalue-count estimate, a
+subspace width m0 and a filter degree K.  Both planners start from the same inputs: the
+KPM moments of the matrix (``kpm_moments``, computed once per matrix on the GPU) and the
+window's bounds mapped to [-1, 1].
+
+Plain rule (the fallback and the judge):
+    N  = KPM count of the window
+    m0 = 1.5 N + 16, rounded up to a multiple of 8
+    K  = ceil(4 pi d / (emax - emin)),  d = (smax - smin) / 2
+(the step filter's Jackson transition width is about pi d / K; a quarter of the window
+separates its edge from the first eigenvalue outside a 1.5 N-wide subspace).
+
+Learned planner: a three-layer perceptron (258 -> 256 -> 256 -> 3, BF16 weights, FP32
+arithmetic, trained on the GPU by the library's own kernels) maps [mu_0..mu_255, a, b]
+to (log s_K, log s_m, log s_N), and the plan is K = s_K K_plain, m0 = s_m m0_plain,
+N = s_N N_kpm.  Its training targets come from runs of the plain solver: each training
+window is solved at a grid of (s_K, s_m) scales and the cheapest converged run (fewest
+column-steps, iterations x m0 x (K + 1)) is the target.
+
+:func:`solve_windows` runs the learned plan and re-solves, with the plain rule, every
+window that did not converge or returned clearly fewer eigenvalues than the KPM count
+predicts.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from typing import Iterable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib as L
+from .api import _op_of, kpm_moments, kpm_count, slice_spectrum
+
+N_MOMENTS = 256
+IN_DIM = N_MOMENTS + 2
+HIDDEN = 256
+OUT_DIM = 3
+SCALE_GRID_K = (0.25, 0.35, 0.5, 0.7, 1.0)
+SCALE_GRID_M = (1.0, 1.5, 2.2)
+_CLIP = (math.log(0.2), math.log(3.0))
+WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "planner_data", "planner_weights.npz")
+
+
+# ---------------------------------------------------------------------- features and rules
+def mapped(smin: float, smax: float, e: float) -> float:
+    c, d = 0.5 * (smin + smax), 0.5 * (smax - smin)
+    return (e - c) / d
+
+
+def window_features(mu: np.ndarray, smin: float, smax: float, emin: float, emax: float) -> np.ndarray:
+    """The planner's input row: 256 KPM moments and the window's mapped bounds (float32)."""
+    f = np.zeros(IN_DIM, dtype=np.float32)
+    m = np.asarray(mu, dtype=np.float64)[:N_MOMENTS]
+    f[:m.size] = m
+    f[N_MOMENTS] = mapped(smin, smax, emin)
+    f[N_MOMENTS + 1] = mapped(smin, smax, emax)
+    return f
+
+
+def plain_rule(count: float, smin: float, smax: float, emin: float, emax: float) -> Tuple[int, int]:
+    """(degree, m0) of the plain rule for a window holding about ``count`` eigenvalues."""
+    d = 0.5 * (smax - smin)
+    K = int(math.ceil(4.0 * math.pi * d / (emax - emin)))
+    m0 = int(8 * math.ceil((1.5 * max(count, 1.0) + 16.0) / 8.0))
+    return K, m0
+
+
+def scaled(K: int, m0: int, sK: float, sm: float, n: int) -> Tuple[int, int]:
+    return max(1, int(round(K * sK))), min(n // 8 * 8, int(8 * math.ceil(m0 * sm / 8.0)))
+
+
+# ---------------------------------------------------------------------- the network
+class WindowPlanner:
+    """The learned planner's network on the GPU (``sma_mlp_*``)."""
+
+    def __init__(self, seed: int = 0, ctx=None, in_dim: int = IN_DIM, hidden: int = HIDDEN,
+                 out_dim: int = OUT_DIM):
+        from .api import context
+
+        self.ctx = ctx or context()
+        self.in_dim, self.hidden, self.out_dim = in_dim, hidden, out_dim
+        h = ctypes.c_void_p()
+        L.check(L.load().sma_mlp_create(self.ctx.handle, in_dim, hidden, out_dim, int(seed),
+                                        ctypes.byref(h)))
+        self.handle = h
+        cnt = ctypes.c_int64()
+        L.check(L.load().sma_mlp_num_params(h, ctypes.byref(cnt)))
+        self.num_params = cnt.value
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                L.load().sma_mlp_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+    @property
+    def params(self) -> np.ndarray:
+        p = np.empty(self.num_params, dtype=np.float32)
+        L.check(L.load().sma_mlp_get_params(self.handle, p.ctypes.data))
+        return p
+
+    @params.setter
+    def params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != self.num_params:
+            raise ValueError(f"expected {self.num_params} parameters, got {p.size}")
+        L.check(L.load().sma_mlp_set_params(self.handle, p.ctypes.data))
+
+    def forward(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32).reshape(-1, self.in_dim)
+        Y = np.empty((X.shape[0], self.out_dim), dtype=np.float32)
+        L.check(L.load().sma_mlp_forward(self.handle, X.ctypes.data, X.shape[0], Y.ctypes.data))
+        return Y
+
+    def grad(self, X, T, w=None):
+        X = np.ascontiguousarray(X, dtype=np.float32).reshape(-1, self.in_dim)
+        T = np.ascontiguousarray(T, dtype=np.float32).reshape(-1, self.out_dim)
+        wp = None if w is None else np.ascontiguousarray(w, dtype=np.float32).reshape(T.shape)
+        g = np.empty(self.num_params, dtype=np.float32)
+        loss = ctypes.c_float()
+        L.check(L.load().sma_mlp_grad(self.handle, X.ctypes.data, T.ctypes.data,
+                                      None if wp is None else wp.ctypes.data, X.shape[0],
+                                      ctypes.byref(loss), g.ctypes.data))
+        return loss.value, g
+
+    def train(self, X, T, w=None, steps: int = 2000, lr: float = 1e-3, minibatch: int = 64,
+              seed: int = 0, weight_decay: float = 1e-4) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32).reshape(-1, self.in_dim)
+        T = np.ascontiguousarray(T, dtype=np.float32).reshape(-1, self.out_dim)
+        wp = None if w is None else np.ascontiguousarray(w, dtype=np.float32).reshape(T.shape)
+        hist = np.empty(max(int(steps), 1), dtype=np.float32)
+        L.check(L.load().sma_mlp_train(self.handle, X.ctypes.data, T.ctypes.data,
+                                       None if wp is None else wp.ctypes.data, X.shape[0],
+                                       int(steps), float(lr), int(minibatch), int(seed),
+                                       float(weight_decay), hist.ctypes.data))
+        return hist[:int(steps)]
+
+    def save(self, path: str) -> None:
+        np.savez_compressed(path, params=self.params, in_dim=self.in_dim, hidden=self.hidden,
+                            out_dim=self.out_dim)
+
+    @classmethod
+    def load(cls, path: str = WEIGHTS, ctx=None) -> "WindowPlanner":
+        z = np.load(path)
+        net = cls(ctx=ctx, in_dim=int(z["in_dim"]), hidden=int(z["hidden"]), out_dim=int(z["out_dim"]))
+        net.params = z["params"]
+        return net
+
+
+# ---------------------------------------------------------------------- planning and solving
+def plan_windows(A, windows: Sequence[Tuple[float, float]], planner: Optional[WindowPlanner] = None,
+                 mu: Optional[np.ndarray] = None, smin=None, smax=None):
+    """Per window: (count estimate, degree, m0), by the learned planner when given, else
+    by the plain rule.  Returns the three lists and the plain rule's (degree, m0)."""
+    op = _op_of(A)
+    if smin is None or smax is None:
+        smin, smax = op.gershgorin_bounds()
+    if mu is None:
+        mu = kpm_moments(op, N_MOMENTS, 16, smin=smin, smax=smax)
+    counts, plain = [], []
+    for a, b in windows:
+        N = kpm_count(mu, op.n, smin, smax, a, b)
+        counts.append(N)
+        plain.append(plain_rule(N, smin, smax, a, b))
+    if planner is None:
+        return counts, [k for k, _ in plain], [m for _, m in plain], plain
+    X = np.stack([window_features(mu, smin, smax, a, b) for a, b in windows])
+    Y = np.clip(planner.forward(X), *_CLIP)
+    deg, m0, cnt = [], [], []
+    for (K, m), N, y in zip(plain, counts, Y):
+        k2, m2 = scaled(K, m, math.exp(y[0]), math.exp(y[1]), op.n)
+        deg.append(k2)
+        m0.append(m2)
+        cnt.append(N * math.exp(y[2]))
+    return cnt, deg, m0, plain
+
+
+def window_cost(iterations, m0, degree) -> np.ndarray:
+    """Column-steps of a window's solve: iterations x m0 x (K + 1)."""
+    return np.asarray(iterations) * np.asarray(m0) * (np.asarray(degree) + 1)
+
+
+def solve_windows(A, windows, planner: Optional[WindowPlanner] = None, *, smin=None, smax=None,
+                  mu=None, maxiter: int = 10, precision: str = "fp64", tol: float = 1e-10,
+                  seed: int = 1, report: Optional[dict] = None):
+    """Batched slicing with a planned (degree, m0) per window.  With a planner, windows
+    that did not converge, or returned fewer than 0.85 N - 3 eigenvalues of the KPM count
+    N, are solved again with the plain rule.  Returns ``(lam, X, res, win)`` like
+    :func:`slice_spectrum`; ``report`` receives the plans, per-window column-steps and the
+    windows redone."""
+    op = _op_of(A)
+    if smin is None or smax is None:
+        smin, smax = op.gershgorin_bounds()
+    if mu is None:
+        mu = kpm_moments(op, N_MOMENTS, 16, smin=smin, smax=smax)
+    counts, deg, m0, plain = plan_windows(op, windows, planner, mu, smin, smax)
+    st = {}
+    lam, X, res, win = slice_spectrum(op, windows, deg, m0, smin=smin, smax=smax, maxiter=maxiter,
+                                      precision=precision, tol=tol, seed=seed, stats=st)
+    cost = window_cost(st["window_iterations"], m0, deg)
+    kpm_n = [kpm_count(mu, op.n, smin, smax, a, b) for a, b in windows]
+    redo = []
+    if planner is not None:
+        for w in range(len(windows)):
+            got = int(np.sum(win == w))
+            if not st["window_converged"][w] or got < 0.85 * kpm_n[w] - 3:
+                redo.append(w)
+    if redo:
+        st2 = {}
+        sub = [windows[w] for w in redo]
+        l2, X2, r2, w2 = slice_spectrum(op, sub, [plain[w][0] for w in redo],
+                                        [plain[w][1] for w in redo], smin=smin, smax=smax,
+                                        maxiter=maxiter, precision=precision, tol=tol, seed=seed,
+                                        stats=st2)
+        cost2 = window_cost(st2["window_iterations"], [plain[w][1] for w in redo],
+                            [plain[w][0] for w in redo])
+        keep = ~np.isin(win, redo)
+        parts = [(lam[keep], X[:, keep], res[keep], win[keep])]
+        for j, w in enumerate(redo):
+            s = w2 == j
+            parts.append((l2[s], X2[:, s], r2[s], np.full(int(s.sum()), w)))
+            cost[w] += cost2[j]
+        order_w = np.concatenate([p[3] for p in parts])
+        lam_c = np.concatenate([p[0] for p in parts])
+        perm = np.lexsort((lam_c, order_w))
+        lam = lam_c[perm]
+        X = np.concatenate([p[1] for p in parts], axis=1)[:, perm]
+        res = np.concatenate([p[2] for p in parts])[perm]
+        win = order_w[perm]
+    if report is not None:
+        report.update(dict(degree=deg, m0=m0, count_estimate=counts, plain=plain, cost=cost,
+                           redone=redo, kpm_count=kpm_n, iterations=st["window_iterations"]))
+    return lam, X, res, win
+
+
+# ---------------------------------------------------------------------- training data
+def training_rows(A, windows, *, smin=None, smax=None, mu=None, maxiter: int = 10, seed: int = 1,
+                  grid_k: Iterable[float] = SCALE_GRID_K, grid_m: Iterable[float] = SCALE_GRID_M):
+    """Rows (features, targets, weights) from runs of the plain solver on ``A``: every
+    window is solved once per (s_K, s_m) of the grid, all in ONE batched slicing call; the
+    target is the cheapest converged scale pair, and log(found / KPM count) where the most
+    generous run converged.  Windows with no converged run get zero weight."""
+    op = _op_of(A)
+    if smin is None or smax is None:
+        smin, smax = op.gershgorin_bounds()
+    if mu is None:
+        mu = kpm_moments(op, N_MOMENTS, 16, smin=smin, smax=smax)
+    grid = [(sk, sm) for sk in grid_k for sm in grid_m]
+    wins, deg, m0, owner = [], [], [], []
+    plans = []
+    for wi, (a, b) in enumerate(windows):
+        N = kpm_count(mu, op.n, smin, smax, a, b)
+        K, m = plain_rule(N, smin, smax, a, b)
+        plans.append((N, K, m))
+        for sk, sm in grid:
+            k2, m2 = scaled(K, m, sk, sm, op.n)
+            wins.append((a, b))
+            deg.append(k2)
+            m0.append(m2)
+            owner.append(wi)
+    st = {}
+    lam, X, res, win = slice_spectrum(op, wins, deg, m0, smin=smin, smax=smax, maxiter=maxiter,
+                                      seed=seed, stats=st)
+    nrm = max(abs(smin), abs(smax))
+    cost = window_cost(st["window_iterations"], m0, deg)
+    F, T, W = [], [], []
+    for wi, (a, b) in enumerate(windows):
+        N, K, m = plans[wi]
+        idx = [j for j in range(len(wins)) if owner[j] == wi]
+        found = [int(np.sum((win == j) & (res <= 1e-10 * nrm))) for j in idx]
+        ref = max(found)  # the most eigenvalues any converged run found
+        ok = [j for jj, j in enumerate(idx) if st["window_converged"][j] and found[jj] == ref and ref > 0]
+        f = window_features(mu, smin, smax, a, b)
+        if not ok:
+            F.append(f); T.append(np.zeros(OUT_DIM, np.float32)); W.append(np.zeros(OUT_DIM, np.float32))
+            continue
+        best = min(ok, key=lambda j: cost[j])
+        g = grid[idx.index(best)]
+        F.append(f)
+        T.append(np.array([math.log(g[0]), math.log(g[1]), math.log(max(ref, 1) / max(N, 1.0))],
+                          np.float32))
+        W.append(np.ones(OUT_DIM, np.float32))
+    return np.stack(F), np.stack(T), np.stack(W)
+
+
+# ---------------------------------------------------------------------- window placement
+def energy_at_count(mu, n: int, smin: float, smax: float, start: float, count: float,
+                    hi: Optional[float] = None) -> float:
+    """The energy e > start with ``count`` KPM-estimated eigenvalues in [start, e]
+    (bisection; the estimate is monotone up to KPM ripple)."""
+    lo_e, hi_e = start, smax if hi is None else hi
+    for _ in range(80):
+        mid = 0.5 * (lo_e + hi_e)
+        if kpm_count(mu, n, smin, smax, start, mid) < count:
+            lo_e = mid
+        else:
+            hi_e = mid
+    return 0.5 * (lo_e + hi_e)
+
+
+def windows_by_count(mu, n: int, smin: float, smax: float, center: float,
+                     counts: Sequence[float]) -> List[Tuple[float, float]]:
+    """Contiguous windows whose KPM-estimated counts are ``counts``, the whole run
+    centred on ``center``."""
+    total = float(sum(counts))
+    # start so that about half of the total lies below the centre
+    lo_e, hi_e = smin, center
+    for _ in range(80):
+        mid = 0.5 * (lo_e + hi_e)
+        if kpm_count(mu, n, smin, smax, mid, center) > 0.5 * total:
+            lo_e = mid
+        else:
+            hi_e = mid
+    e = 0.5 * (lo_e + hi_e)
+    out = []
+    for c in counts:
+        e2 = energy_at_count(mu, n, smin, smax, e, c)
+        out.append((e, e2))
+        e = e2
+    return out

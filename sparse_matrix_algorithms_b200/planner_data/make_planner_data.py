@@ -1,0 +1,148 @@
+"""Training data and weights of the learned window planner.
+
+    python -m sparse_matrix_algorithms_b200.planner_data.make_planner_data gen   # -> planner_train.npz
+    python -m sparse_matrix_algorithms_b200.planner_data.make_planner_data train # -> planner_weights.npz
+
+``gen`` draws matrices from the two model families -- 3D Anderson (L in 12..20, W uniform
+in [2, 20]) and the XXZ chain (L in 12..16, h uniform in [0.5, 8]) -- places windows of
+12..64 KPM-estimated eigenvalues in the bulk of each spectrum, and solves every window at
+the grid of (degree, width) scales of the plain rule in one batched slicing call per
+matrix (``planner.training_rows``).  ``train`` fits the network on the GPU with the
+library's own kernels.  Needs a GPU.  Matrices are smaller than the sizes the planner is
+meant to serve; the features (KPM moments and mapped window bounds) do not depend on n.
+"""
+import argparse
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from sparse_matrix_algorithms_b200 import api as S  # noqa: E402
+from sparse_matrix_algorithms_b200 import matrices as M  # noqa: E402
+from sparse_matrix_algorithms_b200 import planner as P  # noqa: E402
+
+
+def sample_matrix(rng):
+    if rng.uniform() < 0.6:
+        L = int(rng.choice([12, 14, 16, 18, 20]))
+        W = float(rng.uniform(2.0, 20.0))
+        seed = int(rng.integers(1 << 30))
+        return f"anderson L={L} W={W:.3f} seed={seed}", M.anderson3d(L, W, seed)
+    L = int(rng.choice([12, 14, 16]))
+    h = float(rng.uniform(0.5, 8.0))
+    seed = int(rng.integers(1 << 30))
+    return f"xxz L={L} h={h:.3f} seed={seed}", M.xxz_sz0(L, h, seed)
+
+
+def sample_windows(rng, mu, n, smin, smax, k):
+    # window centres between the 15% and 85% points of the KPM cumulative count
+    lo = P.energy_at_count(mu, n, smin, smax, smin, 0.15 * n)
+    hi = P.energy_at_count(mu, n, smin, smax, smin, 0.85 * n)
+    out = []
+    for _ in range(k):
+        c = float(rng.uniform(lo, hi))
+        N = float(rng.uniform(12, 64))
+        w = P.windows_by_count(mu, n, smin, smax, c, [N])[0]
+        out.append(w)
+    return out
+
+
+def gen(args):
+    rng = np.random.default_rng(args.seed)
+    F, T, W, names = [], [], [], []
+    t0 = time.time()
+    for i in range(args.matrices):
+        name, A = sample_matrix(rng)
+        op = S.SparseOperator(A)
+        smin, smax = op.gershgorin_bounds()
+        mu = S.kpm_moments(op, P.N_MOMENTS, 16, smin=smin, smax=smax)
+        wins = sample_windows(rng, mu, A.shape[0], smin, smax, args.windows)
+        f, t, w = P.training_rows(op, wins, smin=smin, smax=smax, mu=mu)
+        F.append(f); T.append(t); W.append(w); names += [name] * len(wins)
+        print(f"{i + 1}/{args.matrices} {name}: {int(w[:, 0].sum())}/{len(wins)} windows usable, "
+              f"{time.time() - t0:.1f} s", flush=True)
+    np.savez_compressed(args.out, X=np.concatenate(F), T=np.concatenate(T), W=np.concatenate(W),
+                        names=np.array(names))
+
+
+def train(args):
+    z = np.load(args.data)
+    net = P.WindowPlanner(seed=args.seed)
+    hist = net.train(z["X"], z["T"], z["W"], steps=args.steps, lr=args.lr,
+                     minibatch=args.minibatch, seed=args.seed, weight_decay=args.weight_decay)
+    print(f"loss {hist[:20].mean():.4f} -> {hist[-20:].mean():.4f}")
+    net.save(args.out)
+
+
+HELD_OUT = [("anderson", 14, 12.0, 77), ("anderson", 18, 4.0, 78), ("xxz", 14, 3.0, 79),
+            ("xxz", 12, 6.5, 80)]
+
+
+def held_out_problem(kind, L, p, seed):
+    return M.anderson3d(L, p, seed) if kind == "anderson" else M.xxz_sz0(L, p, seed)
+
+
+def evaluate(weights=P.WEIGHTS, problems=HELD_OUT, counts=(20, 45, 30), verbose=True):
+    """Column-steps of the plain rule and of the learned plan (fallback re-solves
+    included) on held-out matrices; also whether both found the same eigenvalues."""
+    net = P.WindowPlanner.load(weights)
+    rows = []
+    for kind, L, p, seed in problems:
+        A = held_out_problem(kind, L, p, seed)
+        op = S.SparseOperator(A)
+        smin, smax = op.gershgorin_bounds()
+        nrm = max(abs(smin), abs(smax))
+        mu = S.kpm_moments(op, P.N_MOMENTS, 16, smin=smin, smax=smax)
+        centre = P.energy_at_count(mu, A.shape[0], smin, smax, smin, 0.5 * A.shape[0])
+        wins = P.windows_by_count(mu, A.shape[0], smin, smax, centre, counts)
+        rp, rl = {}, {}
+        lp, _, resp, wp = P.solve_windows(op, wins, None, smin=smin, smax=smax, mu=mu, report=rp)
+        ll, _, resl, wl = P.solve_windows(op, wins, net, smin=smin, smax=smax, mu=mu, report=rl)
+        same = lp.size == ll.size and bool(np.all(wp == wl)) and (
+            lp.size == 0 or float(np.abs(lp - ll).max()) <= 1e-12 * nrm)
+        row = dict(problem=f"{kind} L={L} p={p} seed={seed}", plain=int(np.sum(rp["cost"])),
+                   learned=int(np.sum(rl["cost"])), redone=len(rl["redone"]), same=same,
+                   found=int(lp.size), maxres=float(max(resp.max(), resl.max()) / nrm) if lp.size else None,
+                   plain_deg=rp["degree"], learned_deg=rl["degree"], plain_m0=rp["m0"],
+                   learned_m0=rl["m0"])
+        rows.append(row)
+        if verbose:
+            print(row, flush=True)
+    return rows
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    g = sub.add_parser("gen")
+    g.add_argument("--matrices", type=int, default=32)
+    g.add_argument("--windows", type=int, default=4)
+    g.add_argument("--seed", type=int, default=2024)
+    g.add_argument("--out", default=os.path.join(HERE, "planner_train.npz"))
+    t = sub.add_parser("train")
+    t.add_argument("--data", default=os.path.join(HERE, "planner_train.npz"))
+    t.add_argument("--steps", type=int, default=3000)
+    t.add_argument("--lr", type=float, default=1e-3)
+    t.add_argument("--minibatch", type=int, default=32)
+    t.add_argument("--weight-decay", type=float, default=1e-3)
+    t.add_argument("--seed", type=int, default=7)
+    t.add_argument("--out", default=P.WEIGHTS)
+    e = sub.add_parser("eval")
+    e.add_argument("--weights", default=P.WEIGHTS)
+    a = ap.parse_args()
+    if a.cmd == "gen":
+        gen(a)
+    elif a.cmd == "train":
+        train(a)
+    else:
+        rows = evaluate(a.weights)
+        tp, tl = sum(r["plain"] for r in rows), sum(r["learned"] for r in rows)
+        print(f"column-steps: plain {tp}, learned {tl}, ratio {tp / tl:.2f}")
+
+
+if __name__ == "__main__":
+    main()
