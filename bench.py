@@ -1,23 +1,35 @@
-"""Benchmark: eigenpairs/s of POLFED on the XXZ L=18 workload, plus SpMM GB/s.
+"""Benchmark: eigenpairs/s of POLFED in FP64, chosen configuration vs plain, plus SpMM GB/s.
 
-Workload (one "step" = one full solve): plain POLFED in FP64 on the random-field XXZ
-chain L=18, periodic, J=Delta=1, h_i ~ U[-5, 5] (seed 1), Sz=0 sector (n=48620,
-~10.5 nnz/row); the 200 eigenvalues nearest the spectral centre; block size s=32.
-The window [emin, emax] holds exactly those 200 eigenvalues of the dense FP64
-spectrum (tests/golden/xxz_L18_spectrum.npz); its ends sit at mid-gaps.
+Default workload (one "step" = one full solve) -- the C2 configuration: POLFED in FP64 on
+the random-field XXZ chain L=18, periodic, J=Delta=1, h_i ~ U[-5, 5] (seed 1), Sz=0
+sector (n=48620, ~10.5 nnz/row); the 200 eigenvalues nearest the spectral centre; block
+size s=32, mmax=24.  The window [emin, emax] holds exactly those 200 eigenvalues of the
+dense FP64 spectrum (tests/golden/xxz_L18_spectrum.npz); its ends sit at mid-gaps.
+
+Two arms per step, both FP64 POLFED through the library:
+  plain   Gershgorin bounds, degree 2200 (the smallest degree of the sweep with which all
+          200 pairs converge);
+  chosen  Lanczos spectral bounds (100 GPU Lanczos steps, INSIDE the timed step) and the
+          degree scaled by the ratio of the two half-widths, which keeps the filter's
+          resolution in eigenvalue units (2200 -> ~1780).
+value is the chosen arm; plain_fp64 is the plain arm in the same run.
+
+--workload c3: the 3D Anderson model L=64 (n=262144), W=16.5, seed 2; 500 eigenvalues in
+a window centred at E=0 placed by KPM (256 moments, 32 vectors) and fixed; s=64,
+mmax=22, degree 12 d / (emax - emin) for either arm's half-width d.
 
 value     eigenpairs with relative residual ||Ax-lam x||/||A|| <= 1e-10 found inside the
           window, per second of device time (CUDA events on the library's stream),
           matrix resident in HBM; L2 flushed (256 MiB write) before every solve.
-e2e       the same metric through the public API with host buffers: CSR upload, solve,
-          eigenvector download inside the timed region.
+e2e       the chosen arm through the public API with host buffers: CSR upload, bounds,
+          solve, eigenvector download inside the timed region.
 roofline  the fused Clenshaw-SpMM step: algorithmic bytes of all filter launches
           (12 nnz + 4(n+1) + 32 n b per step, FP64) / device time of the filter phases,
           against the measured HBM copy bandwidth.
 With --gpus N under torchrun every rank runs an independent replica (the path has no
 data exchange); value is the sum over ranks, timed as the max over ranks.
 --impl reference times the CPU restatement of the reference algorithm (oracle/) on a
-bounded sample of the same workload on all host cores.
+bounded sample of the plain arm on all host cores.
 """
 from __future__ import annotations
 
@@ -36,44 +48,81 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "eigenpairs/s at residual<=1e-10: chosen vs plain FP64 on one B200; SpMM GB/s"
-# Degree and basis size: the smallest pair of the sweep {600..2200} x {14, 18, 24} with
-# which every one of the 200 pairs reaches residual <= 1e-10 ||A|| (the reference's rule:
-# raise the degree until converged, chebyshev_subspace_iteration.jl:1051).
-NEV, S_BLOCK, DEGREE, MMAX, WINDOW = 200, 32, 2200, 24, "delta"
-CPU_COLUMNS = 8  # columns of a block the CPU sample filters (the others are identical work)
-# dram__bytes_read.sum + dram__bytes_write.sum of one fused Clenshaw step on this workload
-# (ncu --set full, one launch; profiles/clenshaw_step_xxz_L18_b32_fp64.md)
-TRAFFIC_BYTES_PER_STEP = 43_698_688 + 242_944
+WINDOW = "delta"
+LANCZOS_STEPS = 100
+# dram__bytes_read.sum + dram__bytes_write.sum of one fused Clenshaw step of the C2
+# workload (ncu --set full, one launch; profiles/clenshaw_step_xxz_L18_b32_fp64.md)
+TRAFFIC_BYTES_PER_STEP_C2 = 43_698_688 + 242_944
+# the C3 window: 500 eigenvalues by the KPM estimate (256 moments, 32 Rademacher vectors,
+# seed 11, Gershgorin bounds) centred at E=0, fixed here
+C3_WINDOW = (-0.016975627263859053, 0.016979915488252416)
 
 
-def c2_workload():
-    from sparse_matrix_algorithms_b200 import matrices as M
+class Workload:
+    """Matrix, window, POLFED sizes and the plain degree of one benchmark configuration."""
 
-    A = M.config_matrix("xxz_L18")
-    g = np.load(os.path.join(ROOT, "tests", "golden", "xxz_L18_spectrum.npz"))
-    lam_min, lam_max = float(g["lam_min"]), float(g["lam_max"])
-    central = g["central"]
-    centre = 0.5 * (lam_min + lam_max)
-    order = np.argsort(np.abs(central - centre), kind="stable")[:NEV]
-    lo, hi = int(order.min()), int(order.max())
-    emin = 0.5 * (central[lo - 1] + central[lo])
-    emax = 0.5 * (central[hi] + central[hi + 1])
-    exact = central[lo:hi + 1]
-    norm = max(abs(lam_min), abs(lam_max))
-    return A, dict(emin=emin, emax=emax, sigma=0.5 * (emin + emax), exact=exact, norm=norm)
+    def __init__(self, name):
+        from sparse_matrix_algorithms_b200 import matrices as M
 
+        self.name = name
+        if name == "c2":
+            self.A = M.config_matrix("xxz_L18")
+            g = np.load(os.path.join(ROOT, "tests", "golden", "xxz_L18_spectrum.npz"))
+            lam_min, lam_max = float(g["lam_min"]), float(g["lam_max"])
+            central = g["central"]
+            centre = 0.5 * (lam_min + lam_max)
+            self.nev, self.s, self.mmax = 200, 32, 24
+            order = np.argsort(np.abs(central - centre), kind="stable")[:self.nev]
+            lo, hi = int(order.min()), int(order.max())
+            self.emin = 0.5 * (central[lo - 1] + central[lo])
+            self.emax = 0.5 * (central[hi] + central[hi + 1])
+            self.exact_count = hi - lo + 1
+            self.norm = max(abs(lam_min), abs(lam_max))
+            self.norm_kind = "dense FP64 spectrum"
+            # the smallest degree of the sweep {600..2200} x mmax {14, 18, 24} with which
+            # every pair reaches residual <= 1e-10 ||A|| (the reference's rule: raise the
+            # degree until converged, chebyshev_subspace_iteration.jl:1051)
+            self.degree_plain = 2200
+            self.cpu_columns = 8
+            self.traffic = TRAFFIC_BYTES_PER_STEP_C2
+            self.text = ("C2 POLFED FP64: XXZ L=18 Sz=0 periodic (n=48620), J=Delta=1, "
+                         "h~U[-5,5] seed 1; 200 eigenvalues nearest the spectral centre; s=32")
+        elif name == "c3":
+            self.A = M.config_matrix("anderson_L64")
+            self.nev, self.s, self.mmax = 500, 64, 22
+            self.emin, self.emax = C3_WINDOW
+            gold = os.path.join(ROOT, "tests", "golden", "anderson_L64_near0.npz")
+            self.exact_count = None
+            if os.path.exists(gold):
+                lam = np.load(gold)["near"]
+                self.exact_count = int(np.sum((lam >= self.emin) & (lam <= self.emax)))
+            self.norm = None  # from the Lanczos bounds at set-up
+            self.norm_kind = "Lanczos estimate"
+            from sparse_matrix_algorithms_b200.api import gershgorin_bounds
+            gl, gh = gershgorin_bounds(self.A)
+            self.degree_plain = int(12 * 0.5 * (gh - gl) / (self.emax - self.emin))
+            self.cpu_columns = 1
+            self.traffic = None
+            self.text = ("C3 POLFED FP64: 3D Anderson L=64 (n=262144), W=16.5, seed 2, periodic; "
+                         "500 eigenvalues (KPM-placed window centred at E=0); s=64")
+        else:
+            raise ValueError(name)
+        self.sigma = 0.5 * (self.emin + self.emax)
 
-def polfed_kwargs(A, w):
-    from sparse_matrix_algorithms_b200.api import gershgorin_bounds
+    def kwargs(self, smin, smax):
+        return dict(s=self.s, smin=smin, smax=smax, sigma=self.sigma, emin=self.emin,
+                    emax=self.emax, tol=1e-10, window_type=WINDOW, mmax=self.mmax)
 
-    smin, smax = gershgorin_bounds(A)
-    return dict(s=S_BLOCK, smin=smin, smax=smax, sigma=w["sigma"], emin=w["emin"],
-                emax=w["emax"], tol=1e-10, window_type=WINDOW, mmax=MMAX)
+    def good_pairs(self, lam, res):
+        inside = (lam >= self.emin) & (lam <= self.emax)
+        return int(np.count_nonzero(inside & (res <= 1e-10 * self.norm)))
 
-
-def good_pairs(lam, res, w):
-    inside = (lam >= w["emin"]) & (lam <= w["emax"])
-    return int(np.count_nonzero(inside & (res <= 1e-10 * w["norm"])))
+    def config(self):
+        return {"workload": self.text, "window": WINDOW, "mmax": self.mmax,
+                "degree_plain": self.degree_plain, "bounds_plain": "Gershgorin",
+                "bounds_chosen": f"Lanczos ({LANCZOS_STEPS} steps, in the timed step)",
+                "exact_count_in_window": self.exact_count, "norm": self.norm_kind,
+                "l2": "flushed before every solve (256 MiB write)", "parallelism": "replicas"}
 
 
 class ClockSampler:
@@ -129,25 +178,28 @@ def measured_hbm_peak():
     return 6650.0, "fallback"
 
 
-def cpu_sample(A, w, kw, threads):
-    """Oracle (CPU restatement) estimate of one POLFED block, in seconds: the Clenshaw
-    filter of degree DEGREE timed on CPU_COLUMNS of the block's S_BLOCK columns (each
-    column's recurrence is independent, identical work) and scaled to the block, plus the
-    timed reorthogonalization and QR of a full mid-run block, on all host cores.  A solve
-    is MMAX such blocks; the extraction is not counted (it favours the CPU)."""
+def cpu_sample(wl: Workload, threads: int, max_degree: int = 0):
+    """Oracle (CPU restatement) estimate of one plain-arm POLFED block, in seconds: the
+    Clenshaw filter timed on ``wl.cpu_columns`` of the block's s columns (each column's
+    recurrence is independent, identical work) and scaled to the block -- and, when
+    ``max_degree`` truncates the recurrence, scaled from the steps run to the full degree
+    -- plus the timed reorthogonalization and QR of a full mid-run block, on all host
+    cores.  A solve is mmax such blocks; the extraction is not counted (it favours the
+    CPU)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import sma_oracle as O
     from sparse_matrix_algorithms_b200 import matrices as M
 
+    A = wl.A
     n = A.shape[0]
-    coeffs = O.build_coeffs(DEGREE, kw["smin"], kw["smax"], kw["sigma"], kw["emin"], kw["emax"],
-                            WINDOW, True)
-    Q = O.orth_block(M.splitmix_normal(1, n, S_BLOCK))
-    V = np.linalg.qr(M.splitmix_normal(2, n, S_BLOCK * MMAX // 2))[0]
+    smin, smax = O.gershgorin_bounds(A)
+    K = wl.degree_plain if not max_degree else min(max_degree, wl.degree_plain)
+    coeffs = O.build_coeffs(K, smin, smax, wl.sigma, wl.emin, wl.emax, WINDOW, True)
+    Q = O.orth_block(M.splitmix_normal(1, n, wl.s))
+    V = np.linalg.qr(M.splitmix_normal(2, n, wl.s * wl.mmax // 2))[0]
     t0 = time.perf_counter()
-    O.apply_poly_block(A, Q[:, :CPU_COLUMNS], coeffs, kw["smin"], kw["smax"], impl="c",
-                       nthreads=threads)
-    t_filter = (time.perf_counter() - t0) * (S_BLOCK / CPU_COLUMNS)
+    O.apply_poly_block(A, Q[:, :wl.cpu_columns], coeffs, smin, smax, impl="c", nthreads=threads)
+    t_filter = (time.perf_counter() - t0) * (wl.s / wl.cpu_columns) * (wl.degree_plain / K)
     W = Q.copy()
     t1 = time.perf_counter()
     W -= V @ (V.T @ W)  # the reorthogonalization of a mid-run block
@@ -155,152 +207,171 @@ def cpu_sample(A, w, kw, threads):
     return t_filter + (time.perf_counter() - t1)
 
 
+def _cpu_text(wl: Workload, max_degree: int) -> str:
+    trunc = (f", recurrence truncated to {max_degree} steps and scaled to {wl.degree_plain}"
+             if max_degree and max_degree < wl.degree_plain else "")
+    return (f"one POLFED block of the CPU restatement (oracle/clenshaw_ref.c filter of degree "
+            f"{wl.degree_plain} timed on {wl.cpu_columns} of the {wl.s} columns and scaled{trunc}; "
+            f"the block's reorthogonalization and QR) x {wl.mmax} blocks; extraction not counted; "
+            f"credited with the {wl.nev} pairs the full solve finds")
+
+
+CPU_MAX_DEGREE = {"c2": 0, "c3": 400}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    A, w = c2_workload()
-    from sparse_matrix_algorithms_b200 import matrices  # noqa: F401
-
-    kw = _host_kwargs(A, w)
+    wl = Workload(args.workload)
     threads = os.cpu_count() or 1
+    md = CPU_MAX_DEGREE[wl.name]
     for _ in range(args.warmup):
-        cpu_sample(A, w, kw, threads)
-    t = [cpu_sample(A, w, kw, threads) for _ in range(args.steps)]
+        cpu_sample(wl, threads, md)
+    t = [cpu_sample(wl, threads, md) for _ in range(args.steps)]
     t_block = sum(t) / len(t)
-    solve_s = t_block * MMAX
-    value = NEV / solve_s
+    value = wl.nev / (t_block * wl.mmax)
     line = {
         "metric": METRIC, "impl": "reference", "value": value, "unit": "eigenpairs/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * t_block, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": _config(),
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": wl.config(),
         "cpu_baseline": {"value": value, "unit": "eigenpairs/s", "cores": threads, "kind": "port",
-                         "sample": f"per step one POLFED block on the CPU restatement: "
-                                   f"oracle/clenshaw_ref.c filter of degree {DEGREE} timed on "
-                                   f"{CPU_COLUMNS} of the {S_BLOCK} columns and scaled, plus the "
-                                   f"block's reorthogonalization and QR; solve time = {MMAX} blocks "
-                                   f"(extraction not counted); credited with the {NEV} pairs the "
-                                   f"full solve finds"},
+                         "sample": "per step " + _cpu_text(wl, md)},
         "e2e": {"value": value, "unit": "eigenpairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
-
-
-def _host_kwargs(A, w):
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import sma_oracle as O
-
-    smin, smax = O.gershgorin_bounds(A)
-    return dict(smin=smin, smax=smax, sigma=w["sigma"], emin=w["emin"], emax=w["emax"])
-
-
-def _config():
-    return {"workload": "C2 plain POLFED FP64: XXZ L=18 Sz=0 periodic (n=48620), J=Delta=1, "
-                        "h~U[-5,5] seed 1; 200 eigenvalues nearest the spectral centre; s=32",
-            "degree": DEGREE, "mmax": MMAX, "window": WINDOW, "bounds": "Gershgorin",
-            "l2": "flushed before every solve (256 MiB write)", "parallelism": "replicas"}
 
 
 def run_ours(args, rank, world, device):
     import torch
 
     import sparse_matrix_algorithms_b200 as S
+    from sparse_matrix_algorithms_b200 import _lib as L
 
-    A, w = c2_workload()
+    wl = Workload(args.workload)
+    A = wl.A
     ctx = S.context(device)
     op = S.SparseOperator(A, ctx)
-    kw = polfed_kwargs(A, w)
+    gl, gh = op.gershgorin_bounds()
+    if wl.norm is None:
+        lo, hi = S.lanczos_bounds(op, steps=LANCZOS_STEPS)
+        wl.norm = max(abs(lo), abs(hi))
     stream = torch.cuda.ExternalStream(ctx.stream, device=device)
     flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=device)
+    lib = L.load()
 
-    def solve(stats=None):
-        return S.polfed(op, NEV, DEGREE, stats=stats, **kw)
+    def plain(stats=None):
+        return S.polfed(op, wl.nev, wl.degree_plain, stats=stats, **wl.kwargs(gl, gh))
 
-    for _ in range(args.warmup):
-        solve()
-    torch.cuda.synchronize(device)
-    if world > 1:
-        torch.distributed.barrier()
-    pairs, step_ms, agg = 0, [], {"filter_bytes": 0.0, "filter_ms": 0.0, "kernel_launches": 0,
-                                   "spmm_steps": 0}
-    with ClockSampler(device) as clk:
-        for _ in range(args.steps):
+    def chosen(stats=None, operator=None):
+        o = operator or op
+        lo, hi = S.lanczos_bounds(o, steps=LANCZOS_STEPS)
+        K = int(round(wl.degree_plain * (hi - lo) / (gh - gl)))
+        if stats is not None:
+            stats["degree"] = K
+        return S.polfed(o, wl.nev, K, stats=stats, **wl.kwargs(lo, hi))
+
+    def timed(fn, steps):
+        pairs, ms, launches = 0, [], 0
+        agg = {"filter_bytes": 0.0, "filter_ms": 0.0}
+        degree = None
+        for _ in range(steps):
             flush.zero_()
             torch.cuda.synchronize(device)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            l0 = lib.sma_kernel_launch_count()
             e0.record(stream)
             st = {}
-            lam, X, res = solve(st)
+            lam, X, res = fn(st)
             e1.record(stream)
             e1.synchronize()
-            step_ms.append(e0.elapsed_time(e1))
-            pairs += good_pairs(lam, res, w)
+            launches += lib.sma_kernel_launch_count() - l0
+            ms.append(e0.elapsed_time(e1))
+            pairs += wl.good_pairs(lam, res)
             for k in agg:
                 agg[k] += st[k]
-        torch.cuda.synchronize(device)
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms, pairs], dtype=torch.float64, device=device)
-        tmax = t.clone()
-        torch.distributed.all_reduce(tmax[:1], op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(t[1:], op=torch.distributed.ReduceOp.SUM)
-        total_ms, pairs = float(tmax[0]), int(t[1])
-    value = pairs / (total_ms / 1e3)
+            degree = st.get("degree")
+        return pairs, sum(ms), agg, launches, degree
 
-    # end to end through the public API with host buffers
+    for _ in range(args.warmup):
+        plain()
+        chosen()
+    torch.cuda.synchronize(device)
+    if world > 1:
+        torch.distributed.barrier()
+    with ClockSampler(device) as clk:
+        c_pairs, c_ms, c_agg, c_launch, c_deg = timed(chosen, args.steps)
+        torch.cuda.synchronize(device)
+    p_pairs, p_ms, p_agg, _, _ = timed(plain, args.steps)
+    if world > 1:
+        t = torch.tensor([c_ms, p_ms, c_pairs, p_pairs], dtype=torch.float64, device=device)
+        tmax = t.clone()
+        torch.distributed.all_reduce(tmax, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+        c_ms, p_ms, c_pairs, p_pairs = float(tmax[0]), float(tmax[1]), int(t[2]), int(t[3])
+    value = c_pairs / (c_ms / 1e3)
+    plain_value = p_pairs / (p_ms / 1e3)
+
+    # end to end through the public API with host buffers: upload, bounds, solve, download
     e2e_ms, e2e_pairs = [], 0
     h2d = 8 * (A.shape[0] + 1) + 16 * A.nnz
     d2h = 0
-    for _ in range(max(1, min(args.steps, 3))):
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
         flush.zero_()
         torch.cuda.synchronize(device)
         t0 = time.perf_counter()
-        lam, X, res = S.polfed(A, NEV, DEGREE, **kw)
+        hop = S.SparseOperator(A, ctx)
+        lam, X, res = chosen(None, hop)
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
-        e2e_pairs += good_pairs(lam, res, w)
+        e2e_pairs += wl.good_pairs(lam, res)
         d2h = 8 * (X.size + lam.size + res.size)
+        hop.close()
     e2e = {"value": e2e_pairs / (sum(e2e_ms) / 1e3), "unit": "eigenpairs/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "timing": "host wall clock around the API call, device synchronized"}
+           "timing": "host wall clock around the API calls, device synchronized"}
 
     if rank != 0:
         return
     peak, peak_kind = measured_hbm_peak()
-    achieved = agg["filter_bytes"] / (agg["filter_ms"] / 1e3) / 1e9
-    traffic = TRAFFIC_BYTES_PER_STEP
+    achieved = c_agg["filter_bytes"] / (c_agg["filter_ms"] / 1e3) / 1e9
     cpu = None
     if world == 1:
-        hk = _host_kwargs(A, w)
         threads = os.cpu_count() or 1
-        t_block = cpu_sample(A, w, hk, threads)
-        cpu = {"value": NEV / (t_block * MMAX), "unit": "eigenpairs/s", "cores": threads,
-               "kind": "port",
-               "sample": f"one POLFED block of the CPU restatement (filter degree {DEGREE} "
-                         f"timed on {CPU_COLUMNS} of {S_BLOCK} columns and scaled, "
-                         f"reorthogonalization, QR) x {MMAX} blocks; extraction not counted"}
+        md = CPU_MAX_DEGREE[wl.name]
+        t_block = cpu_sample(wl, threads, md)
+        cpu = {"value": wl.nev / (t_block * wl.mmax), "unit": "eigenpairs/s", "cores": threads,
+               "kind": "port", "sample": _cpu_text(wl, md)}
+    cfg = wl.config()
+    cfg["degree_chosen"] = c_deg
     line = {
         "metric": METRIC, "value": value, "unit": "eigenpairs/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": c_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": _config(),
-        "pairs_per_step": pairs / args.steps / world,
+        "data": "synthetic", "config": cfg,
+        "pairs_per_step": c_pairs / args.steps / world,
+        "plain_fp64": {"value": plain_value, "unit": "eigenpairs/s",
+                       "ms_per_step": p_ms / args.steps,
+                       "pairs_per_step": p_pairs / args.steps / world,
+                       "spmm_gbs": p_agg["filter_bytes"] / (p_agg["filter_ms"] / 1e3) / 1e9},
+        "chosen_vs_plain": value / plain_value if plain_value > 0 else None,
         "spmm_gbs": achieved,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
-                     "kernel": "clenshaw_step_kernel (fused CSR SpMM + Clenshaw axpy)",
+                     "frac": achieved / peak, "traffic": wl.traffic,
+                     "kernel": "fused CSR Clenshaw step (SpMM + recurrence axpy)",
                      "peak_kind": f"{peak_kind} HBM copy bandwidth",
-                     "note": "working set (~56 MB) is L2-resident at this size"},
+                     "note": ("working set (~56 MB) is L2-resident at this size"
+                              if wl.name == "c2" else "blocks of 134 MB per step exceed L2")},
         "e2e": e2e,
-        "gpu_launches": agg["kernel_launches"],
+        "gpu_launches": c_launch,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
 
 
-def run_profile_filter(prec: str, width: int, degree: int, calls: int):
-    """Only the block Clenshaw filter of the benchmark workload on device blocks
+def run_profile_filter(args):
+    """Only the block Clenshaw filter of the workload on device blocks
     (sma_apply_poly_block_dev), `calls` times: the small case for ncu captures of the
     fused step.  Prints the per-step time it measured with CUDA events."""
     import torch
@@ -308,28 +379,29 @@ def run_profile_filter(prec: str, width: int, degree: int, calls: int):
     import sparse_matrix_algorithms_b200 as S
     from sparse_matrix_algorithms_b200 import _lib as L
 
-    A, w = c2_workload()
+    wl = Workload(args.workload)
     ctx = S.context(0)
-    op = S.SparseOperator(A, ctx)
+    op = S.SparseOperator(wl.A, ctx)
     smin, smax = op.gershgorin_bounds()
-    dt = torch.float64 if prec == "fp64" else torch.float32
-    Q = torch.randn(A.shape[0], width, dtype=dt, device="cuda")
+    dt = torch.float64 if args.precision == "fp64" else torch.float32
+    width = args.width or wl.s
+    Q = torch.randn(wl.A.shape[0], width, dtype=dt, device="cuda")
     Y = torch.empty_like(Q)
-    c = np.ascontiguousarray(S.build_coeffs(degree, smin, smax, w["sigma"], w["emin"], w["emax"], WINDOW))
+    c = np.ascontiguousarray(S.build_coeffs(args.degree, smin, smax, wl.sigma, wl.emin, wl.emax, WINDOW))
     stream = torch.cuda.ExternalStream(ctx.stream)
     torch.cuda.synchronize()
     times = []
-    for _ in range(calls):
+    for _ in range(args.calls):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        L.check(L.load().sma_apply_poly_block_dev(op.handle, c.ctypes.data, degree, smin, smax,
+        L.check(L.load().sma_apply_poly_block_dev(op.handle, c.ctypes.data, args.degree, smin, smax,
                                                   Q.data_ptr(), width, Y.data_ptr(), width, width,
-                                                  L.PRECISIONS[prec]))
+                                                  L.PRECISIONS[args.precision]))
         e1.record(stream)
         e1.synchronize()
-        times.append(e0.elapsed_time(e1) / degree)
-    print(json.dumps({"profile_filter": prec, "width": width, "degree": degree,
-                      "us_per_step_last": 1e3 * times[-1]}), flush=True)
+        times.append(e0.elapsed_time(e1) / args.degree)
+    print(json.dumps({"profile_filter": args.precision, "workload": wl.name, "width": width,
+                      "degree": args.degree, "us_per_step_last": 1e3 * times[-1]}), flush=True)
 
 
 def main():
@@ -338,15 +410,16 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3"])
     ap.add_argument("--profile-filter", action="store_true",
                     help="run only the Clenshaw filter of the workload (for ncu captures)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
-    ap.add_argument("--width", type=int, default=S_BLOCK)
+    ap.add_argument("--width", type=int, default=0, help="block width (default: the workload's s)")
     ap.add_argument("--degree", type=int, default=60)
     ap.add_argument("--calls", type=int, default=3)
     args = ap.parse_args()
     if args.profile_filter:
-        run_profile_filter(args.precision, args.width, args.degree, args.calls)
+        run_profile_filter(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

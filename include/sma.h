@@ -161,6 +161,9 @@ typedef struct sma_slice_opts {
 /* ---------------------------------------------------------------- library, context */
 int sma_abi_version(void);
 const char *sma_last_error(void);
+/* Kernels of this library launched by this process so far (all contexts; graph replays
+ * count every kernel they contain; cuBLAS / cuSOLVER launches are not included). */
+int64_t sma_kernel_launch_count(void);
 int sma_ctx_create(int device, sma_ctx **out);
 int sma_ctx_destroy(sma_ctx *ctx);
 int sma_ctx_synchronize(sma_ctx *ctx);

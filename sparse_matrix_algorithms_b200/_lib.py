@@ -101,6 +101,7 @@ MATBLOCK_FN = ctypes.CFUNCTYPE(c_int, c_void_p, c_void_p, c_void_p, c_int64, c_i
 SIGNATURES = [
     ("sma_abi_version", c_int, []),
     ("sma_last_error", ctypes.c_char_p, []),
+    ("sma_kernel_launch_count", c_int64, []),
     ("sma_ctx_create", c_int, [c_int, ctypes.POINTER(c_void_p)]),
     ("sma_ctx_destroy", c_int, [c_void_p]),
     ("sma_ctx_synchronize", c_int, [c_void_p]),

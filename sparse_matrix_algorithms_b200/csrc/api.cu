@@ -79,6 +79,8 @@ using namespace sma;
 
 extern "C" {
 
+int64_t sma_kernel_launch_count(void) { return g_kernel_launches.load(); }
+
 int sma_abi_version(void) { return SMA_ABI_VERSION; }
 
 const char *sma_last_error(void) { return g_last_error.c_str(); }

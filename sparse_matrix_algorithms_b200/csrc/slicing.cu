@@ -164,7 +164,7 @@ struct Window {
   DevBuf<double> Q, Y, X, Aq, lam_d, res_d, scratch;
   std::vector<double> lam, res;
   bool prev_ok = false, done = false, fp64_phase = false;
-  double prev_maxres = INFINITY;
+  MixedSwitch mixed;
   int64_t iterations = 0;
 };
 
@@ -322,12 +322,9 @@ sma_result *slice_solve(sma_op *op, int64_t nwin, const double *emin, const doub
                (long long)cnt, maxres, fp32_iteration ? " fp32" : "");
         fflush(stdout);
       }
-      if (o.precision == SMA_PREC_MIXED && fp32_iteration) {
-        const bool small = cnt > 0 && maxres < 1e-6 * scale;
-        const bool stalled = cnt > 0 && std::isfinite(x.prev_maxres) && maxres > 0.5 * x.prev_maxres;
-        if (small || stalled || it >= o.maxiter - 2) x.fp64_phase = true;
-      }
-      x.prev_maxres = maxres;
+      if (o.precision == SMA_PREC_MIXED && fp32_iteration &&
+          x.mixed.update(x.lam, x.res, x.emin, x.emax, scale, it >= o.maxiter - 2))
+        x.fp64_phase = true;
       const bool ok = cnt > 0 && maxres < o.tol && !fp32_iteration;
       if (o.two_hit ? (ok && (it == 1 || x.prev_ok)) : ok) x.done = true;
       x.prev_ok = ok;

@@ -160,5 +160,31 @@ inline sma_result *empty_result(sma_ctx *ctx, int64_t n) {
   return r;
 }
 
+// MIXED precision, Chebyshev iteration: the FP32 phase ends when the in-window residuals
+// reach what FP32 filtering can deliver (1e-6 of the spectral scale), when they stop
+// improving (less than a factor 2 over the previous iteration), or when only two
+// iterations remain; later iterations filter in FP64.  The measure is the 90% quantile of
+// the residuals of ALL in-window Ritz pairs (no residual gate: FP32 residuals can sit
+// above the gate, and a few spurious in-window Ritz values must not decide).
+struct MixedSwitch {
+  double prev = INFINITY;
+  // returns true when the filter should move to FP64
+  bool update(const std::vector<double> &lam, const std::vector<double> &res, double emin,
+              double emax, double scale, bool last_two) {
+    std::vector<double> r;
+    for (size_t j = 0; j < lam.size(); ++j)
+      if (lam[j] >= emin && lam[j] <= emax) r.push_back(res[j]);
+    double q = INFINITY;
+    if (!r.empty()) {
+      std::sort(r.begin(), r.end());
+      q = r[std::min(r.size() - 1, (size_t)std::ceil(0.9 * (double)r.size()) - 1)];
+    }
+    const bool small = q < 1e-6 * scale;
+    const bool stalled = std::isfinite(q) && std::isfinite(prev) && q > 0.5 * prev;
+    prev = q;
+    return small || stalled || last_two;
+  }
+};
+
 }  // namespace detail
 }  // namespace sma

@@ -15,19 +15,7 @@ namespace sma {
 
 using namespace detail;
 
-// MIXED precision: the FP32 phase ends when the in-window residuals reach what FP32 filtering
-// can deliver (1e-6 of the spectral scale), when they stop improving (less than a factor 2
-// over the previous iteration), or -- for the sparse overload, which runs a fixed number of
-// iterations -- when only two iterations remain.  Iterations after that filter in FP64.
 namespace {
-
-void mixed_switch(Filter &flt, int64_t cnt, double maxres, double prev_maxres, double scale,
-                  bool last_two) {
-  const bool small = cnt > 0 && maxres < 1e-6 * scale;
-  const bool stalled = cnt > 0 && std::isfinite(prev_maxres) && maxres > 0.5 * prev_maxres;
-  if (small || stalled || last_two) flt.fp64_phase = true;
-}
-
 
 // Chebyshev subspace iteration with locking (sma_cheb_opts.lock = 1, matrix-free overload
 // semantics for termination): the in-window Ritz pairs whose residual is below tol are
@@ -49,7 +37,7 @@ sma_result *cheb_solve_locked(sma_op *op, double emin, double emax, const sma_ch
   std::vector<double> lam, res, lam_lock, res_lock;
   int64_t m = m0, nlock = 0, it = 0;
   bool prev_ok = false;
-  double prev_maxres = INFINITY;
+  MixedSwitch mixed;
   for (it = 1; it <= o.maxiter && m > 0; ++it) {
     const bool fp32_iteration = flt.in_fp32();
     clk.mark(PH_FILTER);
@@ -85,9 +73,10 @@ sma_result *cheb_solve_locked(sma_op *op, double emin, double emax, const sma_ch
              (long long)nlock, maxres);
       fflush(stdout);
     }
-    if (o.precision == SMA_PREC_MIXED && fp32_iteration)
-      mixed_switch(flt, cnt, maxres, prev_maxres, std::max(std::fabs(smin), std::fabs(smax)), false);
-    prev_maxres = maxres;
+    if (o.precision == SMA_PREC_MIXED && fp32_iteration &&
+        mixed.update(lam, res, emin, emax, std::max(std::fabs(smin), std::fabs(smax)),
+                     it >= o.maxiter - 2))
+      flt.fp64_phase = true;
     const bool ok = cnt > 0 && maxres < o.tol && !fp32_iteration;
     if (o.two_hit ? (ok && (it == 1 || prev_ok)) : ok) {
       ++it;
@@ -230,7 +219,7 @@ sma_result *cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts
   PhaseClock clk(st);
   DevBuf<double> Q(n * m0, st), Y(n * m0, st), X(n * m0, st), Aq(m0 * m0, st), lam_d(m0, st),
       res_d(m0, st), scratch;
-  double prev_maxres = INFINITY;
+  MixedSwitch mixed;
   launch_randn(st, n, m0, (uint64_t)o.seed, Q.p, m0);  // Random.seed!(seed); Q=randn(n,m0)
   std::vector<double> lam, res;
   bool prev_ok = false;
@@ -279,10 +268,10 @@ sma_result *cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts
       }
       fflush(stdout);
     }
-    if (o.precision == SMA_PREC_MIXED && fp32_iteration)
-      mixed_switch(flt, cnt, maxres, prev_maxres, std::max(std::fabs(smin), std::fabs(smax)),
-                   !mf && it >= o.maxiter - 2);
-    prev_maxres = maxres;
+    if (o.precision == SMA_PREC_MIXED && fp32_iteration &&
+        mixed.update(lam, res, emin, emax, std::max(std::fabs(smin), std::fabs(smax)),
+                     it >= o.maxiter - 2))
+      flt.fp64_phase = true;
     if (mf) {  // chebyshev_subspace_iteration.jl:827-836
       const bool ok = cnt > 0 && maxres < o.tol && !fp32_iteration;
       if (o.two_hit) {
