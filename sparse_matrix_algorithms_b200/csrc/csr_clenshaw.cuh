@@ -47,32 +47,45 @@ __device__ __forceinline__ void epilogue(T *__restrict__ out, const T (&acc)[V],
   stv<T, V>(out, r);
 }
 
-// acc += sum over the row's entries j in [start, end) of vals[j-off] * B1c[cols[j-off] * ldb]
+// R consecutive entries from j: all R gathers are issued before the first FMA, so R
+// neighbour rows are in flight at once; FMAs in ascending entry order.
+template <typename T, int V, int R>
+__device__ __forceinline__ void chunk(const int *__restrict__ cols, const T *__restrict__ vals,
+                                      int off, int j, const T *__restrict__ B1c, int64_t ldb,
+                                      T (&acc)[V]) {
+  int c[R];
+  T x[R][V], a[R];
+#pragma unroll
+  for (int u = 0; u < R; ++u) c[u] = cols[j + u - off];
+#pragma unroll
+  for (int u = 0; u < R; ++u) ldv<T, V>(B1c + (int64_t)c[u] * ldb, x[u]);
+#pragma unroll
+  for (int u = 0; u < R; ++u) a[u] = vals[j + u - off];
+#pragma unroll
+  for (int u = 0; u < R; ++u)
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] = fma(a[u], x[u][v], acc[v]);
+}
+
+// acc += sum over the row's entries j in [start, end) of vals[j-off] * B1c[cols[j-off] * ldb]:
+// chunks of U, then the r < U remaining entries as ONE chunk of exactly r (a switch over
+// r), so that a row shorter than U -- the 7-entry rows of the Anderson lattice under
+// U = 8 -- still has all its gathers in flight together.
 template <typename T, int V, int U>
 __device__ __forceinline__ void row_product(const int *__restrict__ cols, const T *__restrict__ vals,
                                             int off, int start, int end, const T *__restrict__ B1c,
                                             int64_t ldb, T (&acc)[V]) {
   int j = start;
-  for (; j + U <= end; j += U) {
-    int c[U];
-    T x[U][V], a[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) c[u] = cols[j + u - off];
-#pragma unroll
-    for (int u = 0; u < U; ++u) ldv<T, V>(B1c + (int64_t)c[u] * ldb, x[u]);
-#pragma unroll
-    for (int u = 0; u < U; ++u) a[u] = vals[j + u - off];
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-#pragma unroll
-      for (int v = 0; v < V; ++v) acc[v] = fma(a[u], x[u][v], acc[v]);
-  }
-  for (; j < end; ++j) {
-    T x[V];
-    ldv<T, V>(B1c + (int64_t)cols[j - off] * ldb, x);
-    const T a = vals[j - off];
-#pragma unroll
-    for (int v = 0; v < V; ++v) acc[v] = fma(a, x[v], acc[v]);
+  for (; j + U <= end; j += U) chunk<T, V, U>(cols, vals, off, j, B1c, ldb, acc);
+  switch (end - j) {
+    case 7: if constexpr (U > 7) chunk<T, V, 7>(cols, vals, off, j, B1c, ldb, acc); break;
+    case 6: if constexpr (U > 6) chunk<T, V, 6>(cols, vals, off, j, B1c, ldb, acc); break;
+    case 5: if constexpr (U > 5) chunk<T, V, 5>(cols, vals, off, j, B1c, ldb, acc); break;
+    case 4: if constexpr (U > 4) chunk<T, V, 4>(cols, vals, off, j, B1c, ldb, acc); break;
+    case 3: chunk<T, V, 3>(cols, vals, off, j, B1c, ldb, acc); break;
+    case 2: chunk<T, V, 2>(cols, vals, off, j, B1c, ldb, acc); break;
+    case 1: chunk<T, V, 1>(cols, vals, off, j, B1c, ldb, acc); break;
+    default: break;
   }
 }
 
