@@ -22,8 +22,9 @@ using SparseArrays
 using LinearAlgebra
 
 export chebyshev_poly_real_symm_sparse, polfed, MatrixFreeRealSymOp, DeviceCSR, Lap1dDevice,
-       DeviceMatblock, gershgorin_bounds, jackson_kernel, cheb_delta_coeffs,
-       cheb_window_coeffs, cheb_smooth_window_coeffs
+       AndersonDevice, XXZDevice, DeviceMatblock, gershgorin_bounds, lanczos_bounds,
+       jackson_kernel, cheb_delta_coeffs, cheb_window_coeffs, cheb_smooth_window_coeffs,
+       kpm_moments, kpm_count, slice_spectrum
 
 const libsma = get(ENV, "SMA_LIBRARY", joinpath(@__DIR__, "..", "libsma.so"))
 
@@ -32,9 +33,9 @@ mutable struct ChebOpts
     smin::Float64; smax::Float64; has_bounds::Int64; sigma::Float64
     m0::Int64; degree::Int64; maxiter::Int64; tol::Float64; res_gate::Float64
     jackson::Int64; debug::Int64; two_hit::Int64; seed::Int64; window_type::Int64
-    matrix_free::Int64; precision::Int64; reserved::NTuple{8,Int64}
+    matrix_free::Int64; precision::Int64; lock::Int64; reserved::NTuple{7,Int64}
 end
-ChebOpts() = ChebOpts(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, ntuple(_ -> 0, 8))
+ChebOpts() = ChebOpts(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, ntuple(_ -> 0, 7))
 
 mutable struct PolfedOpts
     s::Int64; smin::Float64; smax::Float64; has_bounds::Int64; sigma::Float64
@@ -44,6 +45,13 @@ mutable struct PolfedOpts
     chunk::Int64; precision::Int64; reserved::NTuple{8,Int64}
 end
 PolfedOpts() = PolfedOpts(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, ntuple(_ -> 0, 8))
+
+mutable struct SliceOpts
+    smin::Float64; smax::Float64; has_bounds::Int64; maxiter::Int64; tol::Float64
+    res_gate::Float64; jackson::Int64; two_hit::Int64; seed::Int64; window_type::Int64
+    precision::Int64; graph::Int64; debug::Int64; reserved::NTuple{8,Int64}
+end
+SliceOpts() = SliceOpts(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, ntuple(_ -> 0, 8))
 
 const SMA_ERR_ARG, SMA_ERR_NONSYMMETRIC, SMA_ERR_INTERVAL = 1, 2, 3
 const SMA_ERR_BOUNDS, SMA_ERR_WINDOW = 8, 9
@@ -59,7 +67,8 @@ end
 
 window_code(w::Symbol) = w === :step ? 0 : w === :delta ? 1 : w === :smooth ? 2 :
     error("Unknown window type: $w")
-precision_code(p::Symbol) = p === :fp64 ? 0 : p === :fp32 ? 1 : throw(ArgumentError("precision must be :fp64 or :fp32"))
+precision_code(p::Symbol) = p === :fp64 ? 0 : p === :fp32 ? 1 : p === :mixed ? 2 :
+    throw(ArgumentError("precision must be :fp64, :fp32 or :mixed"))
 
 # ------------------------------------------------------------------ context
 const CTX = Ref{Ptr{Cvoid}}(C_NULL)
@@ -101,6 +110,34 @@ function Lap1dDevice(n::Int)
     h = Ref{Ptr{Cvoid}}(C_NULL)
     check(ccall((:sma_op_create_lap1d, libsma), Cint, (Ptr{Cvoid}, Int64, Ref{Ptr{Cvoid}}), context(), n, h))
     op = Lap1dDevice(h[], n)
+    finalizer(o -> ccall((:sma_op_destroy, libsma), Cint, (Ptr{Cvoid},), o.handle), op)
+    return op
+end
+
+mutable struct AndersonDevice <: DeviceOperator
+    handle::Ptr{Cvoid}
+    n::Int
+end
+"3D Anderson model on an L^3 periodic lattice (on-site energies eps, hopping t) as a device stencil."
+function AndersonDevice(L::Int, eps::Vector{Float64}; t::Float64=-1.0)
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:sma_op_create_anderson, libsma), Cint, (Ptr{Cvoid}, Int64, Ptr{Float64}, Float64, Ref{Ptr{Cvoid}}),
+                context(), L, eps, t, h))
+    op = AndersonDevice(h[], L^3)
+    finalizer(o -> ccall((:sma_op_destroy, libsma), Cint, (Ptr{Cvoid},), o.handle), op)
+    return op
+end
+
+mutable struct XXZDevice <: DeviceOperator
+    handle::Ptr{Cvoid}
+    n::Int
+end
+"Random-field XXZ chain (even L, periodic) in its Sz = 0 sector as a device stencil."
+function XXZDevice(L::Int, h::Vector{Float64}; J::Float64=1.0, Δ::Float64=1.0)
+    hh = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:sma_op_create_xxz, libsma), Cint, (Ptr{Cvoid}, Int64, Float64, Float64, Ptr{Float64}, Ref{Ptr{Cvoid}}),
+                context(), L, J, Δ, h, hh))
+    op = XXZDevice(hh[], binomial(L, L ÷ 2))
     finalizer(o -> ccall((:sma_op_destroy, libsma), Cint, (Ptr{Cvoid},), o.handle), op)
     return op
 end
@@ -205,10 +242,11 @@ function chebyshev_poly_real_symm_sparse(Ain::SparseMatrixCSC{Float64,Int}, emin
         smin::Union{Float64,Nothing}=nothing, smax::Union{Float64,Nothing}=nothing, σ::Float64=0.0,
         m0::Int=200, degree::Int=80, maxiter::Int=8, tol::Float64=1e-10, res_gate::Float64=1e-6,
         jackson::Bool=true, debug::Bool=false, two_hit::Bool=true, seed::Int=1,
-        window_type::Symbol=:step, precision::Symbol=:fp64)
+        window_type::Symbol=:step, precision::Symbol=:fp64, lock::Bool=false)
     op = DeviceCSR(Ain)
     o = cheb_opts(; smin, smax, σ, m0, degree, maxiter, tol, res_gate, jackson, debug, two_hit,
                   seed, window_type, matrix_free=0, precision)
+    o.lock = lock
     h = Ref{Ptr{Cvoid}}(C_NULL)
     check(ccall((:sma_cheb_solve, libsma), Cint, (Ptr{Cvoid}, Float64, Float64, Ref{ChebOpts}, Ref{Ptr{Cvoid}}),
                 op.handle, emin, emax, o, h))
@@ -220,10 +258,11 @@ function chebyshev_poly_real_symm_sparse(matvec!::F, n::Int, emin::Float64, emax
         smax::Union{Float64,Nothing}=nothing, σ::Float64=0.0, m0::Int=200, degree::Int=80,
         maxiter::Int=8, tol::Float64=1e-10, res_gate::Float64=1e-6, jackson::Bool=true,
         debug::Bool=false, two_hit::Bool=true, seed::Int=1, window_type::Symbol=:step,
-        precision::Symbol=:fp64) where {F,G}
+        precision::Symbol=:fp64, lock::Bool=false) where {F,G}
     A = MatrixFreeRealSymOp(n, matvec!, matblock)
     o = cheb_opts(; smin, smax, σ, m0, degree, maxiter, tol, res_gate, jackson, debug, two_hit,
                   seed, window_type, matrix_free=1, precision)
+    o.lock = lock
     h = Ref{Ptr{Cvoid}}(C_NULL)
     check(ccall((:sma_cheb_solve, libsma), Cint, (Ptr{Cvoid}, Float64, Float64, Ref{ChebOpts}, Ref{Ptr{Cvoid}}),
                 A.dev.handle, emin, emax, o, h))
@@ -257,6 +296,63 @@ end
 function polfed(matvec!::F, n::Int, nev::Int, degree::Int; matblock!::Union{Nothing,G}=nothing, kwargs...) where {F,G}
     Aop = isnothing(matblock!) ? MatrixFreeRealSymOp(n, matvec!) : MatrixFreeRealSymOp(n, matvec!, matblock!)
     return polfed(Aop, nev, degree; kwargs...)
+end
+
+# ------------------------------------------------------------------ extensions
+"Spectral bounds from GPU Lanczos (the reference has only gershgorin_bounds)."
+function lanczos_bounds(op::DeviceOperator; steps::Int=60, seed::Int=7)
+    lo = Ref{Float64}(0); hi = Ref{Float64}(0)
+    check(ccall((:sma_lanczos_bounds, libsma), Cint, (Ptr{Cvoid}, Int64, Int64, Ref{Float64}, Ref{Float64}),
+                op.handle, steps, seed, lo, hi))
+    return lo[], hi[]
+end
+
+"Stochastic KPM moments mu[1:M] of the spectral density on [smin, smax] (R Rademacher vectors)."
+function kpm_moments(op::DeviceOperator, M::Int, R::Int, smin::Float64, smax::Float64; seed::Int=11)
+    mu = Vector{Float64}(undef, M)
+    check(ccall((:sma_kpm_moments, libsma), Cint, (Ptr{Cvoid}, Int64, Int64, Int64, Float64, Float64, Ptr{Float64}, Ptr{Float64}),
+                op.handle, M, R, seed, smin, smax, mu, C_NULL))
+    return mu
+end
+
+"Eigenvalue count in [emin, emax] predicted by KPM moments of an n x n operator."
+function kpm_count(mu::Vector{Float64}, n::Int, smin::Float64, smax::Float64, emin::Float64, emax::Float64; jackson::Bool=true)
+    c = Ref{Float64}(0)
+    check(ccall((:sma_kpm_count, libsma), Cint, (Ptr{Float64}, Int64, Int64, Float64, Float64, Float64, Float64, Int64, Ref{Float64}),
+                mu, length(mu), n, smin, smax, emin, emax, jackson, c))
+    return c[]
+end
+
+"""
+    slice_spectrum(op::DeviceCSR, windows, degrees, m0s; kwargs...) -> (λ, X, res, win)
+
+Batched spectrum slicing: every window (emin, emax) runs Chebyshev subspace iteration with
+its own degree and width; all windows are filtered in ONE batched recurrence per iteration.
+`win[j]` is the (1-based) window of pair j.
+"""
+function slice_spectrum(op::DeviceCSR, windows::Vector{Tuple{Float64,Float64}}, degrees::Vector{Int},
+        m0s::Vector{Int}; smin=nothing, smax=nothing, maxiter::Int=8, tol::Float64=1e-10,
+        res_gate::Float64=1e-6, jackson::Bool=true, two_hit::Bool=true, seed::Int=1,
+        window_type::Symbol=:step, precision::Symbol=:fp64, graph::Bool=true)
+    o = SliceOpts()
+    ccall((:sma_slice_opts_default, libsma), Cvoid, (Ref{SliceOpts},), o)
+    if smin !== nothing && smax !== nothing
+        o.smin = smin; o.smax = smax; o.has_bounds = 1
+    end
+    o.maxiter = maxiter; o.tol = tol; o.res_gate = res_gate; o.jackson = jackson
+    o.two_hit = two_hit; o.seed = seed; o.window_type = window_code(window_type)
+    o.precision = precision_code(precision); o.graph = graph
+    emin = first.(windows); emax = last.(windows)
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:sma_slice_solve, libsma), Cint,
+                (Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Ptr{Int64}, Ptr{Int64}, Ref{SliceOpts}, Ref{Ptr{Cvoid}}),
+                op.handle, length(windows), emin, emax, Int64.(degrees), Int64.(m0s), o, h))
+    k = Ref{Int64}(0); nn = Ref{Int64}(0)
+    check(ccall((:sma_result_count, libsma), Cint, (Ptr{Cvoid}, Ref{Int64}, Ref{Int64}), h[], k, nn))
+    win = Vector{Int64}(undef, k[])
+    k[] > 0 && check(ccall((:sma_result_windows, libsma), Cint, (Ptr{Cvoid}, Ptr{Int64}), h[], win))
+    λ, X, res = take_result(h[])
+    return λ, X, res, win .+ 1
 end
 
 end # module
