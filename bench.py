@@ -271,6 +271,8 @@ def run_ours(args, rank, world, device):
             stats["degree"] = K
         return S.polfed(o, wl.nev, K, stats=stats, **wl.kwargs(lo, hi))
 
+    step_ms = {}
+
     def timed(fn, steps):
         pairs, ms, launches = 0, [], 0
         agg = {"filter_bytes": 0.0, "filter_ms": 0.0}
@@ -291,18 +293,21 @@ def run_ours(args, rank, world, device):
             for k in agg:
                 agg[k] += st[k]
             degree = st.get("degree")
+        step_ms.setdefault(fn.__name__, []).extend(round(m, 1) for m in ms)
         return pairs, sum(ms), agg, launches, degree
 
-    for _ in range(args.warmup):
-        plain()
-        chosen()
-    torch.cuda.synchronize(device)
-    if world > 1:
-        torch.distributed.barrier()
+    # the clock sampler starts before the warm-up: starting nvidia-smi stalls the GPU's
+    # work for about a second, which must not fall into a timed solve
     with ClockSampler(device) as clk:
+        for _ in range(args.warmup):
+            plain()
+            chosen()
+        torch.cuda.synchronize(device)
+        if world > 1:
+            torch.distributed.barrier()
         c_pairs, c_ms, c_agg, c_launch, c_deg = timed(chosen, args.steps)
         torch.cuda.synchronize(device)
-    p_pairs, p_ms, p_agg, _, _ = timed(plain, args.steps)
+        p_pairs, p_ms, p_agg, _, _ = timed(plain, args.steps)
     if world > 1:
         t = torch.tensor([c_ms, p_ms, c_pairs, p_pairs], dtype=torch.float64, device=device)
         tmax = t.clone()
@@ -355,6 +360,7 @@ def run_ours(args, rank, world, device):
                        "pairs_per_step": p_pairs / args.steps / world,
                        "spmm_gbs": p_agg["filter_bytes"] / (p_agg["filter_ms"] / 1e3) / 1e9},
         "chosen_vs_plain": value / plain_value if plain_value > 0 else None,
+        "step_ms": step_ms,
         "spmm_gbs": achieved,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": wl.traffic,

@@ -98,6 +98,8 @@ int sma_ctx_create(int device, sma_ctx **out) {
     ctx->device = device;
     const char *at = std::getenv("SMA_AUTOTUNE");
     ctx->autotune = !(at && std::string(at) == "0");
+    const char *fg = std::getenv("SMA_FILTER_GRAPHS");
+    ctx->filter_graphs = !(fg && std::string(fg) == "0");
     try {
       SMA_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
       SMA_CUBLAS(cublasCreate(&ctx->cublas));

@@ -21,12 +21,26 @@ namespace sma {
 template <typename T>
 void ClenshawWork<T>::ensure(const sma_op *op, int64_t n_, int64_t b, cudaStream_t st) {
   if (n_ == n && b <= bcap && b1.p) return;
+  drop_graph();  // the graph holds the old buffers' addresses
   n = n_;
   bcap = b;
   b1.alloc(n * b, st);
   b2.alloc(n * b, st);
   tmp.alloc(n * b, st);
+  q.release();
+  y.release();
   if (op->kind == OP_MATBLOCK) ax.alloc(n * b, st);
+}
+
+template <typename T>
+void ClenshawWork<T>::drop_graph() {
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  exec = nullptr;
+  graph = nullptr;
+  g_op = nullptr;
+  g_b = -1;
+  g_calls = 0;
 }
 
 double clenshaw_step_bytes(const sma_op *op, int64_t b, int elem_bytes) {
@@ -60,27 +74,33 @@ static void matblock_apply(const sma_op *op, cudaStream_t st, const T *X, T *AX,
   }
 }
 
+// One fused step for device operators: the autotuned CSR launch, or (tuned = false, for
+// graph recording) the operator's cached configuration with no events.
 template <typename T>
-FilterCount apply_poly_block(const sma_op *op, cudaStream_t st, const std::vector<double> &coeffs,
-                             double smin, double smax, const T *Q, int64_t ldq, T *Y, int64_t ldy,
-                             int64_t b, ClenshawWork<T> &work) {
+static void fused_step(const sma_op *op, cudaStream_t st, int64_t b, const T *Q, int64_t ldq,
+                       const T *B1, const T *B2, int64_t ldb, T *out, int64_t ldo, double ck,
+                       double alpha, double beta, bool tuned) {
+  if (!tuned && op->kind == OP_CSR)
+    csr_clenshaw_step_untuned<T>(op, st, b, Q, ldq, B1, B2, ldb, out, ldo, ck, alpha, beta, true);
+  else
+    launch_clenshaw_step<T>(op, st, b, Q, ldq, B1, B2, ldb, out, ldo, ck, alpha, beta, true);
+}
+
+// The launches of one filter (K >= 1); returns the step count and algorithmic bytes.
+template <typename T>
+static FilterCount record_filter(const sma_op *op, cudaStream_t st,
+                                 const std::vector<double> &coeffs, double smin, double smax,
+                                 const T *Q, int64_t ldq, T *Y, int64_t ldy, int64_t b,
+                                 ClenshawWork<T> &work, bool tuned) {
   FilterCount fc;
   const int64_t n = op->n;
   const int64_t K = (int64_t)coeffs.size() - 1;
-  require(K >= 0, SMA_ERR_ARG, "empty coefficient vector");
-  if (n == 0 || b == 0) return fc;
   const double c = 0.5 * (smin + smax);
   const double invd = 2.0 / (smax - smin);
   const double alpha = 2.0 * invd;
   const double beta = -2.0 * c * invd;
   const bool fused = op->kind != OP_MATBLOCK;
   const double blk = (double)n * (double)b * sizeof(T);
-  if (K == 0) {  // no loop: Y = c_0 Q
-    launch_scale_block<T>(st, n, b, Q, ldq, Y, ldy, coeffs[0]);
-    fc.bytes += 2 * blk;
-    return fc;
-  }
-  work.ensure(op, n, b, st);
   T *B1 = work.b1.p, *B2 = work.b2.p, *TMP = work.tmp.p;
   const int64_t ld = b;
   // step K+1 of the reference: B1 = c_K Q (its product multiplies zeros)
@@ -90,8 +110,8 @@ FilterCount apply_poly_block(const sma_op *op, cudaStream_t st, const std::vecto
   const double mat_bytes = clenshaw_step_bytes(op, 0, sizeof(T));
   for (int64_t ci = K - 1; ci >= 1; --ci) {
     if (fused) {
-      launch_clenshaw_step<T>(op, st, b, Q, ldq, B1, b2_zero ? nullptr : B2, ld, TMP, ld,
-                              coeffs[ci], alpha, beta, true);
+      fused_step<T>(op, st, b, Q, ldq, B1, b2_zero ? nullptr : B2, ld, TMP, ld, coeffs[ci], alpha,
+                    beta, tuned);
     } else {
       matblock_apply<T>(op, st, B1, work.ax.p, ld, b);
       launch_clenshaw_axpy<T>(st, n, b, Q, ldq, work.ax.p, ld, B1, b2_zero ? nullptr : B2, ld,
@@ -107,8 +127,8 @@ FilterCount apply_poly_block(const sma_op *op, cudaStream_t st, const std::vecto
   }
   // final step: Y = c_0 Q + invd*A B1 - c*invd*B1 - B2
   if (fused) {
-    launch_clenshaw_step<T>(op, st, b, Q, ldq, B1, b2_zero ? nullptr : B2, ld, Y, ldy, coeffs[0],
-                            invd, -(c * invd), true);
+    fused_step<T>(op, st, b, Q, ldq, B1, b2_zero ? nullptr : B2, ld, Y, ldy, coeffs[0], invd,
+                  -(c * invd), tuned);
   } else {
     matblock_apply<T>(op, st, B1, work.ax.p, ld, b);
     launch_clenshaw_axpy<T>(st, n, b, Q, ldq, work.ax.p, ld, B1, b2_zero ? nullptr : B2, ld, Y,
@@ -116,6 +136,74 @@ FilterCount apply_poly_block(const sma_op *op, cudaStream_t st, const std::vecto
   }
   fc.steps += 1;
   fc.bytes += mat_bytes + (b2_zero ? 3 : 4) * blk;
+  return fc;
+}
+
+// Filters of degree below this run eagerly (launch overhead is then not the question).
+constexpr int64_t kGraphMinDegree = 32;
+
+template <typename T>
+FilterCount apply_poly_block(const sma_op *op, cudaStream_t st, const std::vector<double> &coeffs,
+                             double smin, double smax, const T *Q, int64_t ldq, T *Y, int64_t ldy,
+                             int64_t b, ClenshawWork<T> &work) {
+  FilterCount fc;
+  const int64_t n = op->n;
+  const int64_t K = (int64_t)coeffs.size() - 1;
+  require(K >= 0, SMA_ERR_ARG, "empty coefficient vector");
+  if (n == 0 || b == 0) return fc;
+  if (K == 0) {  // no loop: Y = c_0 Q
+    launch_scale_block<T>(st, n, b, Q, ldq, Y, ldy, coeffs[0]);
+    fc.bytes += 2.0 * (double)n * (double)b * sizeof(T);
+    return fc;
+  }
+  work.ensure(op, n, b, st);
+  if (op->kind == OP_MATBLOCK || K < kGraphMinDegree || !op->ctx->filter_graphs)
+    return record_filter<T>(op, st, coeffs, smin, smax, Q, ldq, Y, ldy, b, work, true);
+  // repeated filter -> CUDA graph on the staging blocks
+  const bool same = work.g_op == op && work.g_b == b && work.g_smin == smin &&
+                    work.g_smax == smax && work.g_coeffs == coeffs;
+  if (!same) {
+    work.drop_graph();
+    work.g_op = op;
+    work.g_b = b;
+    work.g_smin = smin;
+    work.g_smax = smax;
+    work.g_coeffs = coeffs;
+  }
+  work.g_calls += 1;
+  if (work.g_calls == 1)  // first call: eager, so the kernel autotuner sees real steps
+    return record_filter<T>(op, st, coeffs, smin, smax, Q, ldq, Y, ldy, b, work, true);
+  if (!work.q.p) {
+    work.q.alloc(n * work.bcap, st);
+    work.y.alloc(n * work.bcap, st);
+  }
+  launch_copy_block<T, T>(st, n, b, Q, ldq, work.q.p, b);
+  if (!work.exec) {
+    const int64_t l0 = g_kernel_launches.load();
+    SMA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      fc = record_filter<T>(op, st, coeffs, smin, smax, work.q.p, b, work.y.p, b, b, work, false);
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(st, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    SMA_CUDA(cudaStreamEndCapture(st, &work.graph));
+    SMA_CUDA(cudaGraphInstantiate(&work.exec, work.graph, 0));
+    work.g_launches = g_kernel_launches.load() - l0;
+    g_kernel_launches.fetch_sub(work.g_launches);  // counted when the graph runs
+  } else {
+    // step and byte counts of the recorded filter
+    const double blk = (double)n * (double)b * sizeof(T);
+    const double mat_bytes = clenshaw_step_bytes(op, 0, sizeof(T));
+    fc.steps = K;
+    fc.bytes = 2 * blk + (mat_bytes + 3 * blk) + (double)(K - 1) * (mat_bytes + 4 * blk);
+  }
+  SMA_CUDA(cudaGraphLaunch(work.exec, st));
+  g_kernel_launches.fetch_add(work.g_launches);
+  work.replays += 1;
+  launch_copy_block<T, T>(st, n, b, work.y.p, b, Y, ldy);
   return fc;
 }
 

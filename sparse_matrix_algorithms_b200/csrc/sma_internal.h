@@ -93,6 +93,8 @@ struct sma_ctx {
   cusolverDnHandle_t cusolver = nullptr;
   int num_sms = 148;
   bool autotune = true;  // SMA_AUTOTUNE=0 in the environment turns the kernel autotuner off
+  // SMA_FILTER_GRAPHS=0 turns off the CUDA-graph replay of repeated filters (filter.cu)
+  bool filter_graphs = true;
 };
 
 enum op_kind { OP_CSR = 0, OP_LAP1D = 1, OP_MATBLOCK = 2, OP_ANDERSON = 3, OP_XXZ = 4 };
@@ -260,12 +262,28 @@ std::vector<double> build_coeffs(int64_t degree, double smin, double smax, doubl
                                  double emin, double emax, int64_t window_type, bool jackson);
 
 // ------------------------------------------------------------------ filter (filter.cu)
-// Work space of the block Clenshaw recurrence: three n x b blocks (+ AX for matrix-free).
+// Work space of the block Clenshaw recurrence: three n x b blocks (+ AX for matrix-free),
+// and the CUDA graph of a repeated filter: from the second call with the same operator,
+// width, coefficients and bounds, the whole recurrence (on staging blocks q -> y at fixed
+// addresses) is replayed from a graph instead of launched step by step.
 template <typename T>
 struct ClenshawWork {
-  DevBuf<T> b1, b2, tmp, ax;
+  DevBuf<T> b1, b2, tmp, ax, q, y;
   int64_t n = 0, bcap = 0;
+  // graph cache
+  const sma_op *g_op = nullptr;
+  int64_t g_b = -1;
+  double g_smin = 0, g_smax = 0;
+  std::vector<double> g_coeffs;
+  int64_t g_calls = 0, g_launches = 0, replays = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
   void ensure(const sma_op *op, int64_t n_, int64_t b, cudaStream_t st);
+  void drop_graph();
+  ClenshawWork() = default;
+  ClenshawWork(const ClenshawWork &) = delete;
+  ClenshawWork &operator=(const ClenshawWork &) = delete;
+  ~ClenshawWork() { drop_graph(); }
 };
 
 // Y = p(A_hat) Q.  Returns the sparse block products issued and their algorithmic bytes.

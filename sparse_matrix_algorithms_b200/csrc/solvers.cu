@@ -115,6 +115,7 @@ sma_result *cheb_solve_locked(sma_op *op, double emin, double emax, const sma_ch
   stats.spmm_columns = flt.columns * (int64_t)(flt.coeffs.size() > 1 ? flt.coeffs.size() - 1 : 1);
   stats.filter_bytes = flt.total.bytes;
   stats.fp32_filter_calls = flt.fp32_calls;
+  stats.graph_replays = flt.w64.replays + flt.w32.replays;
   stats.locked = nlock;
   stats.filter_ms = ph[PH_FILTER];
   stats.orth_ms = ph[PH_ORTH];
@@ -295,6 +296,7 @@ sma_result *cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts
   stats.spmm_columns = flt.total.steps * m0;
   stats.filter_bytes = flt.total.bytes;
   stats.fp32_filter_calls = flt.fp32_calls;
+  stats.graph_replays = flt.w64.replays + flt.w32.replays;
   stats.filter_ms = ph[PH_FILTER];
   stats.orth_ms = ph[PH_ORTH];
   stats.rr_ms = ph[PH_RR];
@@ -468,6 +470,7 @@ sma_result *polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polf
     stats.spmm_columns = flt.columns * (int64_t)(flt.coeffs.size() > 1 ? flt.coeffs.size() - 1 : 1);
     stats.filter_bytes = flt.total.bytes;
     stats.fp32_filter_calls = flt.fp32_calls;
+    stats.graph_replays = flt.w64.replays + flt.w32.replays;
     stats.filter_ms = ph[PH_FILTER];
     stats.orth_ms = ph[PH_ORTH];
     stats.rr_ms = ph[PH_RR];

@@ -358,3 +358,30 @@ def test_polfed_mixed_precision_xxz(lib_built):
     assert lam.size == 20
     assert np.abs(np.sort(lam) - lam_all[mid - 10:mid + 10]).max() <= 1e-12 * nrm
     assert res.max() <= 1e-10 * nrm
+
+
+def test_filter_graph_replay_is_bit_identical(lib_built, monkeypatch):
+    """POLFED calls the same filter once per block: from the second call the recurrence is
+    replayed from a CUDA graph.  A context with graphs off gives bit-identical results."""
+    import sparse_matrix_algorithms_b200 as S
+
+    A = M.xxz_sz0(14, 5.0, 1)
+    lam_all = np.linalg.eigvalsh(A.toarray())
+    mid = int(np.argmin(np.abs(lam_all - 0.5 * (lam_all[0] + lam_all[-1]))))
+    emin, emax = _window_with_gaps(lam_all, mid - 15, mid + 14)
+    smin, smax = O.gershgorin_bounds(A)
+    kw = dict(s=16, smin=smin, smax=smax, sigma=0.5 * (emin + emax), emin=emin, emax=emax,
+              mmax=8, window_type="delta")
+    st = {}
+    lam, X, res = S.polfed(S.SparseOperator(A), 30, 900, stats=st, **kw)
+    assert st["graph_replays"] == 7
+    monkeypatch.setenv("SMA_FILTER_GRAPHS", "0")
+    ctx = S.Context(0)
+    st0 = {}
+    lam0, X0, res0 = S.polfed(S.SparseOperator(A, ctx), 30, 900, stats=st0, **kw)
+    assert st0["graph_replays"] == 0
+    np.testing.assert_array_equal(lam, lam0)
+    np.testing.assert_array_equal(res, res0)
+    np.testing.assert_array_equal(X, X0)
+    # the same kernels, plus the staging copies in and out of each replay
+    assert st["kernel_launches"] == st0["kernel_launches"] + 2 * 7
