@@ -102,7 +102,9 @@ class Workload:
             gl, gh = gershgorin_bounds(self.A)
             self.degree_plain = int(12 * 0.5 * (gh - gl) / (self.emax - self.emin))
             self.cpu_columns = 1
-            self.traffic = None
+            # dram__bytes_read.sum + dram__bytes_write.sum of one b=64 FP64 step (ncu --set
+            # full; profiles/clenshaw_step_anderson_L64_b64_fp64_and_b768_fp32.md)
+            self.traffic = 429_926_656 + 117_963_264
             self.text = ("C3 POLFED FP64: 3D Anderson L=64 (n=262144), W=16.5, seed 2, periodic; "
                          "500 eigenvalues (KPM-placed window centred at E=0); s=64")
         else:
