@@ -100,6 +100,8 @@ int sma_ctx_create(int device, sma_ctx **out) {
     ctx->autotune = !(at && std::string(at) == "0");
     const char *fg = std::getenv("SMA_FILTER_GRAPHS");
     ctx->filter_graphs = !(fg && std::string(fg) == "0");
+    const char *pe = std::getenv("SMA_PERSISTENT");
+    ctx->persistent = pe && std::string(pe) == "1";
     try {
       SMA_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
       SMA_CUBLAS(cublasCreate(&ctx->cublas));

@@ -157,6 +157,12 @@ FilterCount apply_poly_block(const sma_op *op, cudaStream_t st, const std::vecto
     return fc;
   }
   work.ensure(op, n, b, st);
+  if (op->kind == OP_CSR && op->ctx->persistent && K >= kGraphMinDegree) {
+    if (work.coef.count < (size_t)(K + 1)) work.coef.alloc(K + 1, st);
+    if (!work.barrier.p) work.barrier.alloc(3, st);
+    return persistent_filter<T>(op, st, coeffs, smin, smax, Q, ldq, Y, ldy, b, work.b1.p,
+                                work.b2.p, work.tmp.p, work.coef.p, work.barrier.p);
+  }
   if (op->kind == OP_MATBLOCK || K < kGraphMinDegree || !op->ctx->filter_graphs)
     return record_filter<T>(op, st, coeffs, smin, smax, Q, ldq, Y, ldy, b, work, true);
   // repeated filter -> CUDA graph on the staging blocks

@@ -95,6 +95,8 @@ struct sma_ctx {
   bool autotune = true;  // SMA_AUTOTUNE=0 in the environment turns the kernel autotuner off
   // SMA_FILTER_GRAPHS=0 turns off the CUDA-graph replay of repeated filters (filter.cu)
   bool filter_graphs = true;
+  // SMA_PERSISTENT=1: CSR filters run as one persistent cooperative launch (persistent.cu)
+  bool persistent = false;
 };
 
 enum op_kind { OP_CSR = 0, OP_LAP1D = 1, OP_MATBLOCK = 2, OP_ANDERSON = 3, OP_XXZ = 4 };
@@ -268,7 +270,8 @@ std::vector<double> build_coeffs(int64_t degree, double smin, double smax, doubl
 // addresses) is replayed from a graph instead of launched step by step.
 template <typename T>
 struct ClenshawWork {
-  DevBuf<T> b1, b2, tmp, ax, q, y;
+  DevBuf<T> b1, b2, tmp, ax, q, y, coef;
+  DevBuf<unsigned> barrier;  // persistent filter: arrival count, generation, error flag
   int64_t n = 0, bcap = 0;
   // graph cache
   const sma_op *g_op = nullptr;
@@ -295,6 +298,14 @@ template <typename T>
 FilterCount apply_poly_block(const sma_op *op, cudaStream_t st, const std::vector<double> &coeffs,
                          double smin, double smax, const T *Q, int64_t ldq, T *Y, int64_t ldy,
                          int64_t b, ClenshawWork<T> &work);
+
+// The whole filter as one persistent cooperative launch (CSR operators, K >= 1); same
+// results as apply_poly_block's step-by-step recurrence (persistent.cu).
+template <typename T>
+FilterCount persistent_filter(const sma_op *op, cudaStream_t st, const std::vector<double> &coeffs,
+                              double smin, double smax, const T *Q, int64_t ldq, T *Y, int64_t ldy,
+                              int64_t b, T *buf0, T *buf1, T *buf2, T *coeff_dev,
+                              unsigned *barrier_words);
 
 // AX = A X for FP64 blocks (any operator kind)
 void op_apply(const sma_op *op, cudaStream_t st, const double *X, int64_t ldx, double *Y,
