@@ -91,11 +91,13 @@ class Workload:
             self.A = M.config_matrix("anderson_L64")
             self.nev, self.s, self.mmax = 500, 64, 22
             self.emin, self.emax = C3_WINDOW
-            gold = os.path.join(ROOT, "tests", "golden", "anderson_L64_near0.npz")
+            # exact count by Sylvester inertia at the two window ends
+            # (tests/golden/make_inertia_counts.py -> anderson_L64_inertia.json)
+            gold = os.path.join(ROOT, "tests", "golden", "anderson_L64_inertia.json")
             self.exact_count = None
             if os.path.exists(gold):
-                lam = np.load(gold)["near"]
-                self.exact_count = int(np.sum((lam >= self.emin) & (lam <= self.emax)))
+                below = json.load(open(gold))
+                self.exact_count = below[repr(self.emax)] - below[repr(self.emin)]
             self.norm = None  # from the Lanczos bounds at set-up
             self.norm_kind = "Lanczos estimate"
             from sparse_matrix_algorithms_b200.api import gershgorin_bounds
