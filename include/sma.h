@@ -318,6 +318,12 @@ int sma_mlp_train(sma_mlp *net, const float *X, const float *T, const float *w, 
                   int64_t steps, double lr, int64_t minibatch, int64_t seed,
                   double weight_decay, float *loss_hist);
 
+/* Self-test of the bounded device wait (no counterpart in the reference): launches the
+ * persistent filter's grid barrier with one CTA fewer than it awaits, so the wait must
+ * give up after ~10 ms and report through its error flag.  Returns SMA_OK when the test
+ * observed SMA_ERR_TIMEOUT (stored in *observed) and the context is usable afterwards. */
+int sma_selftest_barrier_timeout(sma_ctx *ctx, int64_t *observed);
+
 /* ---------------------------------------------------------------- results */
 /* k = number of returned pairs, n = vector length. */
 int sma_result_count(const sma_result *r, int64_t *k, int64_t *n);

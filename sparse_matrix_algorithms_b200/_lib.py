@@ -158,6 +158,7 @@ SIGNATURES = [
                              ctypes.POINTER(ctypes.c_float), c_void_p]),
     ("sma_mlp_train", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int64,
                               c_double, c_int64, c_int64, c_double, c_void_p]),
+    ("sma_selftest_barrier_timeout", c_int, [c_void_p, ctypes.POINTER(c_int64)]),
     ("sma_result_count", c_int, [c_void_p, ctypes.POINTER(c_int64), ctypes.POINTER(c_int64)]),
     ("sma_result_copy", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("sma_result_stats", c_int, [c_void_p, ctypes.POINTER(Stats)]),

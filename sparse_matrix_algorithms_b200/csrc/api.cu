@@ -597,6 +597,16 @@ int sma_mlp_train(sma_mlp *net, const float *X, const float *T, const float *w, 
   });
 }
 
+int sma_selftest_barrier_timeout(sma_ctx *ctx, int64_t *observed) {
+  return guarded([&] {
+    require(ctx != nullptr && observed != nullptr, SMA_ERR_ARG, "null argument");
+    DeviceGuard g(ctx->device);
+    *observed = barrier_selftest(ctx);
+    require(*observed == SMA_ERR_TIMEOUT, SMA_ERR_INTERNAL,
+            "the bounded barrier did not report its timeout");
+  });
+}
+
 int sma_result_count(const sma_result *r, int64_t *k, int64_t *n) {
   return guarded([&] {
     require(r != nullptr, SMA_ERR_ARG, "null result");

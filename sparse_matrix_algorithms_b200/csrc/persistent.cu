@@ -280,6 +280,32 @@ FilterCount persistent_filter(const sma_op *op, cudaStream_t st, const std::vect
   return fc;
 }
 
+namespace persist {
+// A grid barrier that can never complete: `expected` CTAs are awaited, fewer are launched.
+__global__ void barrier_selftest_kernel(Barrier bar) {
+  grid_sync(bar);
+}
+}  // namespace persist
+
+// Runs the barrier with one CTA missing and a ~10 ms spin limit; returns SMA_ERR_TIMEOUT
+// when the wait gave up and reported it through the error flag (the expected outcome).
+int barrier_selftest(sma_ctx *ctx) {
+  cudaStream_t st = ctx->stream;
+  DevBuf<unsigned> words(3, st);
+  SMA_CUDA(cudaMemsetAsync(words.p, 0, 3 * sizeof(unsigned), st));
+  const unsigned launched = 2;
+  persist::Barrier bar{words.p, words.p + 1, reinterpret_cast<int *>(words.p + 2), launched + 1,
+                       100000ull};
+  void *args[] = {&bar};
+  SMA_CUDA(cudaLaunchCooperativeKernel((const void *)persist::barrier_selftest_kernel,
+                                       dim3(launched), dim3(persist::kThreads), args, 0, st));
+  SMA_CHECK_LAUNCH();
+  int herr = 0;
+  SMA_CUDA(cudaMemcpyAsync(&herr, words.p + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SMA_CUDA(cudaStreamSynchronize(st));
+  return herr ? SMA_ERR_TIMEOUT : SMA_OK;
+}
+
 template FilterCount persistent_filter<double>(const sma_op *, cudaStream_t, const std::vector<double> &,
                                                double, double, const double *, int64_t, double *,
                                                int64_t, int64_t, double *, double *, double *,

@@ -307,6 +307,9 @@ FilterCount persistent_filter(const sma_op *op, cudaStream_t st, const std::vect
                               int64_t b, T *buf0, T *buf1, T *buf2, T *coeff_dev,
                               unsigned *barrier_words);
 
+// persistent.cu: the bounded grid barrier with a missing CTA; SMA_ERR_TIMEOUT expected
+int barrier_selftest(sma_ctx *ctx);
+
 // AX = A X for FP64 blocks (any operator kind)
 void op_apply(const sma_op *op, cudaStream_t st, const double *X, int64_t ldx, double *Y,
               int64_t ldy, int64_t b);

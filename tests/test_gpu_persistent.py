@@ -59,3 +59,25 @@ def test_persistent_polfed_and_chebyshev_bit_identical(lib_built, monkeypatch):
     for a, b in zip(out[0][:6], out[1][:6]):
         np.testing.assert_array_equal(a, b)
     assert out[0][6] > 0 and out[1][6] == 0  # graphs on the step-by-step path only
+
+
+def test_bounded_barrier_reports_timeout_and_context_survives(lib_built):
+    """Failure detection without a fault: the grid barrier waits for a CTA that was never
+    launched, gives up after its spin limit (~10 ms), sets the error flag and returns; the
+    host reads SMA_ERR_TIMEOUT and the context keeps working."""
+    import ctypes
+
+    import sparse_matrix_algorithms_b200 as S
+    from sparse_matrix_algorithms_b200 import _lib as L
+
+    ctx = S.Context(0)
+    obs = ctypes.c_int64(-1)
+    L.check(L.load().sma_selftest_barrier_timeout(ctx.handle, ctypes.byref(obs)))
+    assert obs.value == L.SMA_ERR_TIMEOUT
+    A = M.anderson3d(8, 16.5, 0)
+    op = S.SparseOperator(A, ctx)
+    smin, smax = op.gershgorin_bounds()
+    Q = M.splitmix_normal(1, A.shape[0], 8)
+    c = S.build_coeffs(50, smin, smax, 0.0, -0.5, 0.5, "step")
+    Y = S.apply_poly_block(op, Q, c, smin, smax)
+    assert np.isfinite(Y).all() and np.abs(Y).max() > 0
