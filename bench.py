@@ -223,6 +223,19 @@ def _cpu_text(wl: Workload, max_degree: int) -> str:
 CPU_MAX_DEGREE = {"c2": 0, "c3": 400}
 
 
+def reduce_over_ranks(c_ms, p_ms, c_pairs, p_pairs, device=None):
+    """Replicas: the job's time is the slowest rank's, its pairs the sum over ranks.  Every
+    rank calls this, in the same order (two all-reduces)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([c_ms, p_ms, c_pairs, p_pairs], dtype=torch.float64, device=device)
+    tmax = t.clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(tmax[0]), float(tmax[1]), int(t[2]), int(t[3])
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -313,11 +326,7 @@ def run_ours(args, rank, world, device):
         torch.cuda.synchronize(device)
         p_pairs, p_ms, p_agg, _, _ = timed(plain, args.steps)
     if world > 1:
-        t = torch.tensor([c_ms, p_ms, c_pairs, p_pairs], dtype=torch.float64, device=device)
-        tmax = t.clone()
-        torch.distributed.all_reduce(tmax, op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
-        c_ms, p_ms, c_pairs, p_pairs = float(tmax[0]), float(tmax[1]), int(t[2]), int(t[3])
+        c_ms, p_ms, c_pairs, p_pairs = reduce_over_ranks(c_ms, p_ms, c_pairs, p_pairs, device)
     value = c_pairs / (c_ms / 1e3)
     plain_value = p_pairs / (p_ms / 1e3)
 
