@@ -423,6 +423,24 @@ def run_profile_filter(args):
                       "degree": args.degree, "us_per_step_last": 1e3 * times[-1]}), flush=True)
 
 
+def run_profile_orth(args):
+    """A short POLFED solve on the C3 matrix (s=64, mmax=8, degree 60): its block
+    orthogonalization and reorthogonalization GEMMs have the shapes of the C3 solve
+    (n=262144, basis up to 512 columns, block 64) -- the small case for ncu captures of the
+    dense part.  Prints the phase times."""
+    import sparse_matrix_algorithms_b200 as S
+
+    wl = Workload("c3")
+    op = S.SparseOperator(wl.A, S.context(0))
+    gl, gh = op.gershgorin_bounds()
+    st = {}
+    kw = wl.kwargs(gl, gh)
+    kw["mmax"] = 8
+    S.polfed(op, 100, 60, stats=st, **kw)
+    print(json.dumps({"profile_orth": "c3", "orth_ms": st["orth_ms"], "rr_ms": st["rr_ms"],
+                      "filter_ms": st["filter_ms"], "basis_dim": st["basis_dim"]}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -432,6 +450,8 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c2", "c3"])
     ap.add_argument("--profile-filter", action="store_true",
                     help="run only the Clenshaw filter of the workload (for ncu captures)")
+    ap.add_argument("--profile-orth", action="store_true",
+                    help="a short C3 POLFED solve for ncu captures of its GEMMs")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--width", type=int, default=0, help="block width (default: the workload's s)")
     ap.add_argument("--degree", type=int, default=60)
@@ -439,6 +459,9 @@ def main():
     args = ap.parse_args()
     if args.profile_filter:
         run_profile_filter(args)
+        return
+    if args.profile_orth:
+        run_profile_orth(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
