@@ -9,14 +9,17 @@ dense FP64 spectrum (tests/golden/xxz_L18_spectrum.npz); its ends sit at mid-gap
 Two arms per step, both FP64 POLFED through the library:
   plain   Gershgorin bounds, degree 2200 (the smallest degree of the sweep with which all
           200 pairs converge);
-  chosen  Lanczos spectral bounds (100 GPU Lanczos steps, INSIDE the timed step) and the
-          degree scaled by the ratio of the two half-widths, which keeps the filter's
-          resolution in eigenvalue units (2200 -> ~1780).
+  chosen  Lanczos spectral bounds (100 GPU Lanczos steps, INSIDE the timed step), no
+          Jackson damping (the sharper delta filter needs a larger Krylov basis but fewer
+          steps in all), degree 700 and mmax 44: the fewest filter steps of a sweep with
+          which all 200 pairs converge.
 value is the chosen arm; plain_fp64 is the plain arm in the same run.
 
 --workload c3: the 3D Anderson model L=64 (n=262144), W=16.5, seed 2; 500 eigenvalues in
 a window centred at E=0 placed by KPM (256 moments, 32 vectors) and fixed; s=64,
-mmax=22, degree 12 d / (emax - emin) for either arm's half-width d.
+mmax=22, plain degree 12 d / (emax - emin) with the Gershgorin half-width d; chosen: Lanczos
+bounds, no Jackson damping, degree 1600, mmax 44 (the fewest steps of a sweep converging
+all 494 pairs).
 
 value     eigenpairs with relative residual ||Ax-lam x||/||A|| <= 1e-10 found inside the
           window, per second of device time (CUDA events on the library's stream),
@@ -83,6 +86,10 @@ class Workload:
             # every pair reaches residual <= 1e-10 ||A|| (the reference's rule: raise the
             # degree until converged, chebyshev_subspace_iteration.jl:1051)
             self.degree_plain = 2200
+            # chosen arm: Lanczos bounds, no Jackson damping; the sweep (degree, mmax) in
+            # {700..1781} x {24..44} (1781/24 with damping) -- the fewest filter steps with
+            # which all 200 pairs converge
+            self.chosen = dict(degree=700, mmax=44, jackson=False)
             self.cpu_columns = 8
             self.traffic = TRAFFIC_BYTES_PER_STEP_C2
             self.text = ("C2 POLFED FP64: XXZ L=18 Sz=0 periodic (n=48620), J=Delta=1, "
@@ -103,6 +110,9 @@ class Workload:
             from sparse_matrix_algorithms_b200.api import gershgorin_bounds
             gl, gh = gershgorin_bounds(self.A)
             self.degree_plain = int(12 * 0.5 * (gh - gl) / (self.emax - self.emin))
+            # chosen arm: Lanczos bounds, no Jackson damping; sweep (degree, mmax) in
+            # {1400..3857} x {22..50}: the fewest filter steps converging all 494 pairs
+            self.chosen = dict(degree=1600, mmax=44, jackson=False)
             self.cpu_columns = 1
             # dram__bytes_read.sum + dram__bytes_write.sum of one b=64 FP64 step (ncu --set
             # full; profiles/clenshaw_step_anderson_L64_b64_fp64_and_b768_fp32.md)
@@ -122,8 +132,10 @@ class Workload:
         return int(np.count_nonzero(inside & (res <= 1e-10 * self.norm)))
 
     def config(self):
-        return {"workload": self.text, "window": WINDOW, "mmax": self.mmax,
+        return {"workload": self.text, "window": WINDOW, "mmax_plain": self.mmax,
                 "degree_plain": self.degree_plain, "bounds_plain": "Gershgorin",
+                "jackson_plain": True, "degree_chosen": self.chosen["degree"],
+                "mmax_chosen": self.chosen["mmax"], "jackson_chosen": self.chosen["jackson"],
                 "bounds_chosen": f"Lanczos ({LANCZOS_STEPS} steps, in the timed step)",
                 "exact_count_in_window": self.exact_count, "norm": self.norm_kind,
                 "l2": "flushed before every solve (256 MiB write)", "parallelism": "replicas"}
@@ -283,10 +295,12 @@ def run_ours(args, rank, world, device):
     def chosen(stats=None, operator=None):
         o = operator or op
         lo, hi = S.lanczos_bounds(o, steps=LANCZOS_STEPS)
-        K = int(round(wl.degree_plain * (hi - lo) / (gh - gl)))
+        kw = wl.kwargs(lo, hi)
+        kw["mmax"] = wl.chosen["mmax"]
+        kw["jackson"] = wl.chosen["jackson"]
         if stats is not None:
-            stats["degree"] = K
-        return S.polfed(o, wl.nev, K, stats=stats, **wl.kwargs(lo, hi))
+            stats["degree"] = wl.chosen["degree"]
+        return S.polfed(o, wl.nev, wl.chosen["degree"], stats=stats, **kw)
 
     step_ms = {}
 
@@ -322,7 +336,7 @@ def run_ours(args, rank, world, device):
         torch.cuda.synchronize(device)
         if world > 1:
             torch.distributed.barrier()
-        c_pairs, c_ms, c_agg, c_launch, c_deg = timed(chosen, args.steps)
+        c_pairs, c_ms, c_agg, c_launch, _ = timed(chosen, args.steps)
         torch.cuda.synchronize(device)
         p_pairs, p_ms, p_agg, _, _ = timed(plain, args.steps)
     if world > 1:
@@ -361,7 +375,6 @@ def run_ours(args, rank, world, device):
         cpu = {"value": wl.nev / (t_block * wl.mmax), "unit": "eigenpairs/s", "cores": threads,
                "kind": "port", "sample": _cpu_text(wl, md)}
     cfg = wl.config()
-    cfg["degree_chosen"] = c_deg
     line = {
         "metric": METRIC, "value": value, "unit": "eigenpairs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": c_ms / args.steps,
