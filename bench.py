@@ -43,6 +43,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -147,7 +148,7 @@ class ClockSampler:
     def __init__(self, device: int):
         self.proc = None
         self.device = device
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"sma_bench_clocks_{os.getpid()}_{device}.csv")
 
     def __enter__(self):
         try:

@@ -13,7 +13,7 @@ Differences from the reference that do not change results
 * ``randn`` (Julia's Xoshiro stream) is not reproducible outside Julia; the random
   start block comes from the documented SplitMix64/Box-Muller generator
   (``sparse_matrix_algorithms_b200.matrices.splitmix_normal``), the same formula the
-  CUDA library evaluates.  Parity is judged on converged eigenpairs.
+  CUDA library evaluates.  Parity is compared on converged eigenpairs.
 * Householder QR and the dense symmetric eigensolves go through numpy's LAPACK
   (``dgeqrf``/``dorgqr``, ``dsyevd``) where Julia's ``qr!``/``eigen`` call
   ``geqrt``/``syevr``: same factorizations, rounding-level differences, eigenvector

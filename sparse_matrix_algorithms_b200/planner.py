@@ -5,7 +5,7 @@ subspace width m0 and a filter degree K.  Both planners start from the same inpu
 KPM moments of the matrix (``kpm_moments``, computed once per matrix on the GPU) and the
 window's bounds mapped to [-1, 1].
 
-Plain rule (the fallback and the judge):
+Plain rule (the fallback, and the arbiter of every learned plan):
     N  = KPM count of the window
     m0 = 1.5 N + 16, rounded up to a multiple of 8
     K  = ceil(4 pi d / (emax - emin)),  d = (smax - smin) / 2
