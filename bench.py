@@ -55,7 +55,7 @@ METRIC = "eigenpairs/s at residual<=1e-10: chosen vs plain FP64 on one B200; SpM
 WINDOW = "delta"
 LANCZOS_STEPS = 100
 # dram__bytes_read.sum + dram__bytes_write.sum of one fused Clenshaw step of the C2
-# workload (ncu --set full, one launch; profiles/clenshaw_step_xxz_L18_b32_fp64.md)
+# workload (ncu --set full of one launch of `bench.py --profile-filter --degree 60`)
 TRAFFIC_BYTES_PER_STEP_C2 = 43_698_688 + 242_944
 # the C3 window: 500 eigenvalues by the KPM estimate (256 moments, 32 Rademacher vectors,
 # seed 11, Gershgorin bounds) centred at E=0, fixed here
@@ -116,7 +116,7 @@ class Workload:
             self.chosen = dict(degree=1600, mmax=44, jackson=False)
             self.cpu_columns = 1
             # dram__bytes_read.sum + dram__bytes_write.sum of one b=64 FP64 step (ncu --set
-            # full; profiles/clenshaw_step_anderson_L64_b64_fp64_and_b768_fp32.md)
+            # full of one launch of `bench.py --profile-filter --workload c3 --width 64`)
             self.traffic = 429_926_656 + 117_963_264
             self.text = ("C3 POLFED FP64: 3D Anderson L=64 (n=262144), W=16.5, seed 2, periodic; "
                          "500 eigenvalues (KPM-placed window centred at E=0); s=64")
