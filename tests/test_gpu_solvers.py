@@ -141,7 +141,10 @@ def test_polfed_xxz_exact_count(lib_built):
     assert np.abs(X.T @ X - np.eye(30)).max() < 1e-10
 
 
-def test_polfed_matches_oracle_same_start_block(lib_built):
+@pytest.mark.parametrize("degree,mmax,jackson", [(600, 12, True), (400, 16, False)])
+def test_polfed_matches_oracle_same_start_block(lib_built, degree, mmax, jackson):
+    """Also without Jackson damping (jackson=false, the undamped series: a sharper filter
+    with Gibbs ripples), which converges here with a smaller degree and a larger basis."""
     import sparse_matrix_algorithms_b200 as S
 
     A = M.anderson3d(9, 16.5, 6)
@@ -150,9 +153,9 @@ def test_polfed_matches_oracle_same_start_block(lib_built):
     emin, emax = _window_with_gaps(lam_all, i0, i0 + 19)
     smin, smax = O.gershgorin_bounds(A)
     kw = dict(s=8, smin=smin, smax=smax, sigma=0.0, emin=emin, emax=emax, window_type="step",
-              mmax=12, tol=1e-10)
-    lam_g, X_g, res_g = S.polfed(A, 20, 600, **kw)
-    lam_o, X_o, res_o = O.polfed(A, 20, 600, **kw)
+              mmax=mmax, tol=1e-10, jackson=jackson)
+    lam_g, X_g, res_g = S.polfed(A, 20, degree, **kw)
+    lam_o, X_o, res_o = O.polfed(A, 20, degree, **kw)
     nrm = _norm2(lam_all)
     assert lam_g.size == lam_o.size == 20
     assert np.abs(lam_g - lam_o).max() < 1e-12 * nrm
