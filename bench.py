@@ -18,8 +18,8 @@ value is the chosen arm; plain_fp64 is the plain arm in the same run.
 --workload c3: the 3D Anderson model L=64 (n=262144), W=16.5, seed 2; 500 eigenvalues in
 a window centred at E=0 placed by KPM (256 moments, 32 vectors) and fixed; s=64,
 mmax=22, plain degree 12 d / (emax - emin) with the Gershgorin half-width d; chosen: Lanczos
-bounds, no Jackson damping, degree 1600, mmax 44 (the fewest steps of a sweep converging
-all 494 pairs).
+bounds, no Jackson damping, step window, degree 1200, mmax 44 (the fewest steps of a sweep
+converging all 494 pairs).
 
 value     eigenpairs with relative residual ||Ax-lam x||/||A|| <= 1e-10 found inside the
           window, per second of device time (CUDA events on the library's stream),
@@ -90,7 +90,7 @@ class Workload:
             # chosen arm: Lanczos bounds, no Jackson damping; the sweep (degree, mmax) in
             # {700..1781} x {24..44} (1781/24 with damping) -- the fewest filter steps with
             # which all 200 pairs converge
-            self.chosen = dict(degree=700, mmax=44, jackson=False)
+            self.chosen = dict(degree=700, mmax=44, jackson=False, window="delta")
             self.cpu_columns = 8
             self.traffic = TRAFFIC_BYTES_PER_STEP_C2
             self.text = ("C2 POLFED FP64: XXZ L=18 Sz=0 periodic (n=48620), J=Delta=1, "
@@ -111,9 +111,10 @@ class Workload:
             from sparse_matrix_algorithms_b200.api import gershgorin_bounds
             gl, gh = gershgorin_bounds(self.A)
             self.degree_plain = int(12 * 0.5 * (gh - gl) / (self.emax - self.emin))
-            # chosen arm: Lanczos bounds, no Jackson damping; sweep (degree, mmax) in
-            # {1400..3857} x {22..50}: the fewest filter steps converging all 494 pairs
-            self.chosen = dict(degree=1600, mmax=44, jackson=False)
+            # chosen arm: Lanczos bounds, no Jackson damping; sweep of (window, degree, mmax)
+            # over delta/step x {1200..3857} x {22..50}: the fewest filter steps converging
+            # all 494 pairs (step window 1200/44; the best delta point was 1600/44)
+            self.chosen = dict(degree=1200, mmax=44, jackson=False, window="step")
             self.cpu_columns = 1
             # dram__bytes_read.sum + dram__bytes_write.sum of one b=64 FP64 step (ncu --set
             # full of one launch of `bench.py --profile-filter --workload c3 --width 64`)
@@ -133,10 +134,11 @@ class Workload:
         return int(np.count_nonzero(inside & (res <= 1e-10 * self.norm)))
 
     def config(self):
-        return {"workload": self.text, "window": WINDOW, "mmax_plain": self.mmax,
+        return {"workload": self.text, "window_plain": WINDOW, "mmax_plain": self.mmax,
                 "degree_plain": self.degree_plain, "bounds_plain": "Gershgorin",
                 "jackson_plain": True, "degree_chosen": self.chosen["degree"],
                 "mmax_chosen": self.chosen["mmax"], "jackson_chosen": self.chosen["jackson"],
+                "window_chosen": self.chosen["window"],
                 "bounds_chosen": f"Lanczos ({LANCZOS_STEPS} steps, in the timed step)",
                 "exact_count_in_window": self.exact_count, "norm": self.norm_kind,
                 "l2": "flushed before every solve (256 MiB write)", "parallelism": "replicas"}
@@ -299,6 +301,7 @@ def run_ours(args, rank, world, device):
         kw = wl.kwargs(lo, hi)
         kw["mmax"] = wl.chosen["mmax"]
         kw["jackson"] = wl.chosen["jackson"]
+        kw["window_type"] = wl.chosen["window"]
         if stats is not None:
             stats["degree"] = wl.chosen["degree"]
         return S.polfed(o, wl.nev, wl.chosen["degree"], stats=stats, **kw)
