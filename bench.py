@@ -458,6 +458,23 @@ def run_profile_orth(args):
                       "filter_ms": st["filter_ms"], "basis_dim": st["basis_dim"]}), flush=True)
 
 
+def run_profile_slice(args):
+    """One iteration of batched slicing on the C3 matrix: four windows around E=0 with
+    degrees 400/300/200/100 and widths 256/192/192/128 (768 columns at the top degree),
+    FP32 -- the segmented Clenshaw step for ncu captures."""
+    import sparse_matrix_algorithms_b200 as S
+
+    wl = Workload("c3")
+    op = S.SparseOperator(wl.A, S.context(0))
+    wins = [(-0.08, -0.04), (-0.04, 0.0), (0.0, 0.04), (0.04, 0.08)]
+    st = {}
+    S.slice_spectrum(op, wins, [400, 300, 200, 100], [256, 192, 192, 128], maxiter=1,
+                     two_hit=False, precision="fp32", graph=False, stats=st)
+    print(json.dumps({"profile_slice": "c3", "filter_ms": st["filter_ms"],
+                      "spmm_steps": st["spmm_steps"], "spmm_columns": st["spmm_columns"],
+                      "gbs": st["filter_bytes"] / st["filter_ms"] / 1e6}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -469,6 +486,8 @@ def main():
                     help="run only the Clenshaw filter of the workload (for ncu captures)")
     ap.add_argument("--profile-orth", action="store_true",
                     help="a short C3 POLFED solve for ncu captures of its GEMMs")
+    ap.add_argument("--profile-slice", action="store_true",
+                    help="one batched slicing iteration on the C3 matrix for ncu captures")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--width", type=int, default=0, help="block width (default: the workload's s)")
     ap.add_argument("--degree", type=int, default=60)
@@ -479,6 +498,9 @@ def main():
         return
     if args.profile_orth:
         run_profile_orth(args)
+        return
+    if args.profile_slice:
+        run_profile_slice(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
