@@ -62,6 +62,17 @@ TRAFFIC_BYTES_PER_STEP_C2 = 43_698_688 + 242_944
 C3_WINDOW = (-0.016975627263859053, 0.016979915488252416)
 
 
+def host_gershgorin(A):
+    """Gershgorin interval of a sparse symmetric matrix, on the host (the benchmark's plain
+    degree must not depend on a GPU, since the CPU reference arm builds the same workload)."""
+    import scipy.sparse as sp
+
+    A = sp.csr_matrix(A)
+    d = A.diagonal()
+    r = np.asarray(abs(A).sum(axis=1)).ravel() - np.abs(d)
+    return float(np.min(d - r)), float(np.max(d + r))
+
+
 class Workload:
     """Matrix, window, POLFED sizes and the plain degree of one benchmark configuration."""
 
@@ -108,8 +119,7 @@ class Workload:
                 self.exact_count = below[repr(self.emax)] - below[repr(self.emin)]
             self.norm = None  # from the Lanczos bounds at set-up
             self.norm_kind = "Lanczos estimate"
-            from sparse_matrix_algorithms_b200.api import gershgorin_bounds
-            gl, gh = gershgorin_bounds(self.A)
+            gl, gh = host_gershgorin(self.A)
             self.degree_plain = int(12 * 0.5 * (gh - gl) / (self.emax - self.emin))
             # chosen arm: Lanczos bounds, no Jackson damping; sweep of (window, degree, mmax)
             # over delta/step x {1200..3857} x {22..50}: the fewest filter steps converging
