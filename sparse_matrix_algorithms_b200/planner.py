@@ -325,3 +325,123 @@ def windows_by_count(mu, n: int, smin: float, smax: float, center: float,
         out.append((e, e2))
         e = e2
     return out
+
+
+# ---------------------------------------------------------------------- POLFED windows
+# The same network shape plans a POLFED solve of one window: its outputs are log-scales of
+# the POLFED plain rule's degree and basis size (mmax blocks of s) and the count correction.
+# POLFED plain rule (Jackson-damped delta filter centred on the window):
+#     N = KPM count,  K = ceil(12 d / (emax - emin)),  mmax = ceil(2.8 N / s)
+# (the reference's default mmax, polfed.jl:1131, and the degree that converged every
+# configuration of this library's POLFED sweeps).
+POLFED_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "planner_data",
+                              "polfed_planner_weights.npz")
+POLFED_GRID_K = (0.4, 0.55, 0.75, 1.0)
+POLFED_GRID_M = (1.0, 1.5, 2.0)
+
+
+def polfed_plain_rule(count: float, smin: float, smax: float, emin: float, emax: float,
+                      s: int) -> Tuple[int, int]:
+    """(degree, mmax) of the POLFED plain rule for a window of about ``count`` eigenvalues."""
+    d = 0.5 * (smax - smin)
+    K = int(math.ceil(12.0 * d / (emax - emin)))
+    mmax = max(2, int(math.ceil(2.8 * max(count, 1.0) / s)))
+    return K, mmax
+
+
+def polfed_cost(K: int, mmax: int, s: int) -> int:
+    """Column-steps of a POLFED filter phase: mmax blocks of s columns, K steps each."""
+    return int(K) * int(mmax) * int(s)
+
+
+def polfed_nev(count: float) -> int:
+    """The nev passed to POLFED for a window of about ``count`` eigenvalues: an upper bound,
+    since POLFED returns at most nev pairs (the basis size still follows ``count``)."""
+    return int(math.ceil(1.2 * max(count, 1.0))) + 2
+
+
+def _polfed_good(lam, res, emin, emax, nrm):
+    return int(np.sum((lam >= emin) & (lam <= emax) & (res <= 1e-10 * nrm)))
+
+
+def solve_polfed_window(A, window, planner: Optional[WindowPlanner] = None, *, s: int = 8,
+                        smin=None, smax=None, mu=None, seed: int = 1,
+                        report: Optional[dict] = None):
+    """POLFED on one window with a planned (nev, degree, mmax): the learned plan when a
+    planner is given, else the plain rule.  A learned plan that returns fewer than
+    0.85 N - 3 converged in-window pairs (N the KPM count) is redone with the plain rule.
+    Returns ``(lam, X, res)``; ``report`` receives the plans, the column-steps spent and
+    whether the window was redone."""
+    from .api import polfed
+
+    op = _op_of(A)
+    if smin is None or smax is None:
+        smin, smax = op.gershgorin_bounds()
+    if mu is None:
+        mu = kpm_moments(op, N_MOMENTS, 16, smin=smin, smax=smax)
+    a, b = window
+    nrm = max(abs(smin), abs(smax))
+    N = kpm_count(mu, op.n, smin, smax, a, b)
+    K0, m0 = polfed_plain_rule(N, smin, smax, a, b, s)
+    nev0 = polfed_nev(N)
+    plan = (nev0, K0, m0)
+    if planner is not None:
+        y = np.clip(planner.forward(window_features(mu, smin, smax, a, b)[None, :])[0], *_CLIP)
+        plan = (max(nev0, polfed_nev(N * math.exp(y[2]))), max(1, int(round(K0 * math.exp(y[0])))),
+                max(2, int(math.ceil(m0 * math.exp(y[1])))))
+
+    def run(nev, K, mmax):
+        return polfed(op, nev, K, s=s, smin=smin, smax=smax, sigma=0.5 * (a + b), emin=a,
+                      emax=b, window_type="delta", mmax=mmax, seed=seed)
+
+    lam, X, res = run(*plan)
+    cost = polfed_cost(plan[1], plan[2], s)
+    redone = False
+    if planner is not None and _polfed_good(lam, res, a, b, nrm) < 0.85 * N - 3:
+        lam, X, res = run(nev0, K0, m0)
+        cost += polfed_cost(K0, m0, s)
+        redone = True
+    if report is not None:
+        report.update(dict(plan=plan, plain=(nev0, K0, m0), cost=cost, redone=redone,
+                           kpm_count=N, good=_polfed_good(lam, res, a, b, nrm)))
+    return lam, X, res
+
+
+def polfed_training_rows(A, windows, *, s: int = 8, smin=None, smax=None, mu=None,
+                         grid_k: Iterable[float] = POLFED_GRID_K,
+                         grid_m: Iterable[float] = POLFED_GRID_M):
+    """Rows (features, targets, weights) from POLFED runs of the plain rule at a grid of
+    (degree, mmax) scales per window: the target is the cheapest run (column-steps) that
+    found as many converged in-window pairs as the best run, and log(found / KPM count)."""
+    from .api import polfed
+
+    op = _op_of(A)
+    if smin is None or smax is None:
+        smin, smax = op.gershgorin_bounds()
+    if mu is None:
+        mu = kpm_moments(op, N_MOMENTS, 16, smin=smin, smax=smax)
+    nrm = max(abs(smin), abs(smax))
+    F, T, W = [], [], []
+    for a, b in windows:
+        N = kpm_count(mu, op.n, smin, smax, a, b)
+        K0, m0 = polfed_plain_rule(N, smin, smax, a, b, s)
+        nev = polfed_nev(N)
+        runs = []
+        for sk in grid_k:
+            for sm in grid_m:
+                K, mm = max(1, int(round(K0 * sk))), max(2, int(math.ceil(m0 * sm)))
+                lam, _, res = polfed(op, nev, K, s=s, smin=smin, smax=smax, sigma=0.5 * (a + b),
+                                     emin=a, emax=b, window_type="delta", mmax=mm)
+                runs.append((sk, sm, polfed_cost(K, mm, s), _polfed_good(lam, res, a, b, nrm)))
+        ref = max(r[3] for r in runs)
+        f = window_features(mu, smin, smax, a, b)
+        ok = [r for r in runs if r[3] == ref and ref > 0]
+        if not ok:
+            F.append(f); T.append(np.zeros(OUT_DIM, np.float32)); W.append(np.zeros(OUT_DIM, np.float32))
+            continue
+        best = min(ok, key=lambda r: r[2])
+        F.append(f)
+        T.append(np.array([math.log(best[0]), math.log(best[1]), math.log(ref / max(N, 1.0))],
+                          np.float32))
+        W.append(np.ones(OUT_DIM, np.float32))
+    return np.stack(F), np.stack(T), np.stack(W)

@@ -2,6 +2,7 @@
 
     python -m sparse_matrix_algorithms_b200.planner_data.make_planner_data gen   # -> planner_train.npz
     python -m sparse_matrix_algorithms_b200.planner_data.make_planner_data train # -> planner_weights.npz
+    ... gen-polfed / train-polfed / eval-polfed: the same for the POLFED planner
 
 ``gen`` draws matrices from the two model families -- 3D Anderson (L in 12..20, W uniform
 in [2, 20]) and the XXZ chain (L in 12..16, h uniform in [0.5, 8]) -- places windows of
@@ -115,6 +116,65 @@ def evaluate(weights=P.WEIGHTS, problems=HELD_OUT, counts=(20, 45, 30), verbose=
     return rows
 
 
+def sample_polfed_matrix(rng):
+    """Smaller matrices for the POLFED sweep: every window is solved 12 times."""
+    if rng.uniform() < 0.6:
+        L = int(rng.choice([10, 12, 14]))
+        W = float(rng.uniform(2.0, 20.0))
+        seed = int(rng.integers(1 << 30))
+        return f"anderson L={L} W={W:.3f} seed={seed}", M.anderson3d(L, W, seed)
+    L = int(rng.choice([12, 14]))
+    h = float(rng.uniform(0.5, 8.0))
+    seed = int(rng.integers(1 << 30))
+    return f"xxz L={L} h={h:.3f} seed={seed}", M.xxz_sz0(L, h, seed)
+
+
+def gen_polfed(args):
+    rng = np.random.default_rng(args.seed)
+    F, T, W, names = [], [], [], []
+    t0 = time.time()
+    for i in range(args.matrices):
+        name, A = sample_polfed_matrix(rng)
+        op = S.SparseOperator(A)
+        smin, smax = op.gershgorin_bounds()
+        mu = S.kpm_moments(op, P.N_MOMENTS, 16, smin=smin, smax=smax)
+        wins = sample_windows(rng, mu, A.shape[0], smin, smax, args.windows)
+        f, t, w = P.polfed_training_rows(op, wins, smin=smin, smax=smax, mu=mu)
+        F.append(f); T.append(t); W.append(w); names += [name] * len(wins)
+        print(f"{i + 1}/{args.matrices} {name}: {int(w[:, 0].sum())}/{len(wins)} windows usable, "
+              f"{time.time() - t0:.1f} s", flush=True)
+    np.savez_compressed(args.out, X=np.concatenate(F), T=np.concatenate(T), W=np.concatenate(W),
+                        names=np.array(names))
+
+
+def evaluate_polfed(weights=P.POLFED_WEIGHTS, problems=HELD_OUT, counts=(30, 50), verbose=True):
+    """Column-steps of POLFED's plain rule and of the learned plan (fallback included) on
+    held-out matrices, and whether both found the same converged eigenvalues."""
+    net = P.WindowPlanner.load(weights)
+    rows = []
+    for kind, L, p, seed in problems:
+        A = held_out_problem(kind, L, p, seed)
+        op = S.SparseOperator(A)
+        smin, smax = op.gershgorin_bounds()
+        nrm = max(abs(smin), abs(smax))
+        mu = S.kpm_moments(op, P.N_MOMENTS, 16, smin=smin, smax=smax)
+        centre = P.energy_at_count(mu, A.shape[0], smin, smax, smin, 0.5 * A.shape[0])
+        for win in P.windows_by_count(mu, A.shape[0], smin, smax, centre, counts):
+            rp, rl = {}, {}
+            lp, _, resp = P.solve_polfed_window(op, win, None, smin=smin, smax=smax, mu=mu, report=rp)
+            ll, _, resl = P.solve_polfed_window(op, win, net, smin=smin, smax=smax, mu=mu, report=rl)
+            gp = np.sort(lp[(lp >= win[0]) & (lp <= win[1]) & (resp <= 1e-10 * nrm)])
+            gl = np.sort(ll[(ll >= win[0]) & (ll <= win[1]) & (resl <= 1e-10 * nrm)])
+            same = gp.size == gl.size and (gp.size == 0 or float(np.abs(gp - gl).max()) <= 1e-12 * nrm)
+            row = dict(problem=f"{kind} L={L} p={p} seed={seed}", window=win, plain=rp["cost"],
+                       learned=rl["cost"], redone=rl["redone"], same=same, found=int(gp.size),
+                       plain_plan=rp["plan"], learned_plan=rl["plan"])
+            rows.append(row)
+            if verbose:
+                print(row, flush=True)
+    return rows
+
+
 def main():
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -133,13 +193,30 @@ def main():
     t.add_argument("--out", default=P.WEIGHTS)
     e = sub.add_parser("eval")
     e.add_argument("--weights", default=P.WEIGHTS)
+    gp = sub.add_parser("gen-polfed")
+    gp.add_argument("--matrices", type=int, default=20)
+    gp.add_argument("--windows", type=int, default=3)
+    gp.add_argument("--seed", type=int, default=4048)
+    gp.add_argument("--out", default=os.path.join(HERE, "polfed_planner_train.npz"))
+    tp_ = sub.add_parser("train-polfed")
+    tp_.add_argument("--data", default=os.path.join(HERE, "polfed_planner_train.npz"))
+    tp_.add_argument("--steps", type=int, default=3000)
+    tp_.add_argument("--lr", type=float, default=1e-3)
+    tp_.add_argument("--minibatch", type=int, default=32)
+    tp_.add_argument("--weight-decay", type=float, default=1e-3)
+    tp_.add_argument("--seed", type=int, default=7)
+    tp_.add_argument("--out", default=P.POLFED_WEIGHTS)
+    ep = sub.add_parser("eval-polfed")
+    ep.add_argument("--weights", default=P.POLFED_WEIGHTS)
     a = ap.parse_args()
     if a.cmd == "gen":
         gen(a)
-    elif a.cmd == "train":
+    elif a.cmd in ("train", "train-polfed"):
         train(a)
+    elif a.cmd == "gen-polfed":
+        gen_polfed(a)
     else:
-        rows = evaluate(a.weights)
+        rows = evaluate(a.weights) if a.cmd == "eval" else evaluate_polfed(a.weights)
         tp, tl = sum(r["plain"] for r in rows), sum(r["learned"] for r in rows)
         print(f"column-steps: plain {tp}, learned {tl}, ratio {tp / tl:.2f}")
 

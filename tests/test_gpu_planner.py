@@ -113,3 +113,18 @@ def test_plain_rule_fallback_redoes_failed_windows(lib_built):
     assert rep["redone"] == [0, 1]
     np.testing.assert_array_equal(win, win0)
     np.testing.assert_allclose(lam, lam0, rtol=0, atol=1e-12 * max(abs(smin), abs(smax)))
+
+
+def test_learned_polfed_plan_beats_plain_rule(lib_built):
+    """The POLFED planner (same network, trained on POLFED runs): on matrices it never saw,
+    its (degree, mmax) plans need fewer filter column-steps than POLFED's plain rule --
+    fallback re-solves included -- and return the same converged in-window eigenvalues."""
+    from sparse_matrix_algorithms_b200.planner_data import make_planner_data as D
+
+    rows = D.evaluate_polfed(problems=[("anderson", 14, 12.0, 77), ("xxz", 14, 3.0, 79)],
+                             verbose=False)
+    for r in rows:
+        assert r["same"] and r["found"] >= 20, r
+    plain = sum(r["plain"] for r in rows)
+    learned = sum(r["learned"] for r in rows)
+    assert learned <= 0.85 * plain, (plain, learned)
