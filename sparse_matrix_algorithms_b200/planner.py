@@ -366,12 +366,12 @@ def _polfed_good(lam, res, emin, emax, nrm):
 
 def solve_polfed_window(A, window, planner: Optional[WindowPlanner] = None, *, s: int = 8,
                         smin=None, smax=None, mu=None, seed: int = 1,
-                        report: Optional[dict] = None):
+                        report: Optional[dict] = None, stats: Optional[dict] = None):
     """POLFED on one window with a planned (nev, degree, mmax): the learned plan when a
     planner is given, else the plain rule.  A learned plan that returns fewer than
     0.85 N - 3 converged in-window pairs (N the KPM count) is redone with the plain rule.
     Returns ``(lam, X, res)``; ``report`` receives the plans, the column-steps spent and
-    whether the window was redone."""
+    whether the window was redone; ``stats`` the solver statistics of the last POLFED run."""
     from .api import polfed
 
     op = _op_of(A)
@@ -392,7 +392,7 @@ def solve_polfed_window(A, window, planner: Optional[WindowPlanner] = None, *, s
 
     def run(nev, K, mmax):
         return polfed(op, nev, K, s=s, smin=smin, smax=smax, sigma=0.5 * (a + b), emin=a,
-                      emax=b, window_type="delta", mmax=mmax, seed=seed)
+                      emax=b, window_type="delta", mmax=mmax, seed=seed, stats=stats)
 
     lam, X, res = run(*plan)
     cost = polfed_cost(plan[1], plan[2], s)
