@@ -179,6 +179,16 @@ void *sma_ctx_stream(sma_ctx *ctx);
 int sma_op_create_csc(sma_ctx *ctx, int64_t n, int64_t nnz, const int64_t *colptr,
                       const int64_t *rowval, const double *nzval, int64_t index_base,
                       int64_t check_symmetric, sma_op **out);
+/* Symmetric half storage (no counterpart in the reference; the "next" item of its CSC
+ * path): the same CSC arguments as sma_op_create_csc, but only the upper triangle
+ * (diagonal included) is kept on the device, about half the entries and indices.  Products
+ * are a row pass plus an atomic scatter of the transposed half, so they agree with full
+ * storage to rounding, not bit for bit; the filter runs as product + axpy.  The lower
+ * triangle is not stored: with check_symmetric != 0 the host verifies a_ij == a_ji first.
+ * Gershgorin bounds come from the full rows.  Not accepted by sma_slice_solve. */
+int sma_op_create_csc_upper(sma_ctx *ctx, int64_t n, int64_t nnz, const int64_t *colptr,
+                            const int64_t *rowval, const double *nzval, int64_t index_base,
+                            int64_t check_symmetric, sma_op **out);
 /* Matrix-free 1D Laplacian tridiag(-1,2,-1) as a device stencil (the reference's
  * lap1d_matblock!, polfed.jl:1209-1219). */
 int sma_op_create_lap1d(sma_ctx *ctx, int64_t n, sma_op **out);

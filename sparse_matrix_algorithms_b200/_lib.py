@@ -108,6 +108,8 @@ SIGNATURES = [
     ("sma_ctx_stream", c_void_p, [c_void_p]),
     ("sma_op_create_csc", c_int, [c_void_p, c_int64, c_int64, c_void_p, c_void_p, c_void_p,
                                   c_int64, c_int64, ctypes.POINTER(c_void_p)]),
+    ("sma_op_create_csc_upper", c_int, [c_void_p, c_int64, c_int64, c_void_p, c_void_p,
+                                        c_void_p, c_int64, c_int64, ctypes.POINTER(c_void_p)]),
     ("sma_op_create_lap1d", c_int, [c_void_p, c_int64, ctypes.POINTER(c_void_p)]),
     ("sma_op_create_anderson", c_int, [c_void_p, c_int64, c_void_p, c_double,
                                        ctypes.POINTER(c_void_p)]),

@@ -105,9 +105,16 @@ class _DeviceOp:
 
 class SparseOperator(_DeviceOp):
     """Device copy of a sparse symmetric matrix (its CSC arrays, which for a symmetric
-    matrix are also its CSR arrays).  ``check_symmetric`` verifies A == A^T exactly."""
+    matrix are also its CSR arrays).  ``check_symmetric`` verifies A == A^T exactly.
+    ``storage="upper"`` keeps only the upper triangle on the device (symmetric half
+    storage, ``sma_op_create_csc_upper``): about half the memory, products equal to full
+    storage up to rounding."""
 
-    def __init__(self, A, ctx: Optional[Context] = None, check_symmetric: bool = False):
+    def __init__(self, A, ctx: Optional[Context] = None, check_symmetric: bool = False,
+                 storage: str = "full"):
+        if storage not in ("full", "upper"):
+            raise ArgumentError(L.SMA_ERR_ARG, "storage must be 'full' or 'upper'")
+        self.storage = storage
         self.ctx = ctx or context()
         C = sp.csc_matrix(A, dtype=np.float64)
         if C.shape[0] != C.shape[1]:
@@ -120,10 +127,17 @@ class SparseOperator(_DeviceOp):
         rowval = np.ascontiguousarray(C.indices, dtype=np.int64)
         nzval = np.ascontiguousarray(C.data, dtype=np.float64)
         h = ctypes.c_void_p()
-        L.check(L.load().sma_op_create_csc(
-            self.ctx.handle, self.n, self.nnz, colptr.ctypes.data, rowval.ctypes.data,
-            nzval.ctypes.data, 0, int(bool(check_symmetric)), ctypes.byref(h)))
+        create = (L.load().sma_op_create_csc if storage == "full"
+                  else L.load().sma_op_create_csc_upper)
+        L.check(create(self.ctx.handle, self.n, self.nnz, colptr.ctypes.data, rowval.ctypes.data,
+                       nzval.ctypes.data, 0, int(bool(check_symmetric)), ctypes.byref(h)))
         self.handle = h
+        if storage == "upper":
+            stored = ctypes.c_int64()
+            L.check(L.load().sma_op_info(self.handle, None, ctypes.byref(stored)))
+            self.nnz_stored = stored.value
+        else:
+            self.nnz_stored = self.nnz
 
     def gershgorin_bounds(self):
         lo, hi = ctypes.c_double(), ctypes.c_double()

@@ -149,6 +149,34 @@ int sma_ctx_synchronize(sma_ctx *ctx) {
 
 void *sma_ctx_stream(sma_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
+// Validates CSC arrays on the host (so that no device kernel can index out of bounds) and
+// returns them 0-based as int32 (rp: n+1 column pointers, ci: nnz row indices).
+static void validate_csc(int64_t n, int64_t nnz, const int64_t *colptr, const int64_t *rowval,
+                         const double *nzval, int64_t index_base, std::vector<int> &rp,
+                         std::vector<int> &ci) {
+  require(n >= 0 && nnz >= 0, SMA_ERR_ARG, "negative size");
+  require(n < INT32_MAX && nnz < INT32_MAX, SMA_ERR_ARG, "matrix too large for 32-bit indices");
+  require(index_base == 0 || index_base == 1, SMA_ERR_ARG, "index_base must be 0 or 1");
+  require(colptr != nullptr && (nnz == 0 || (rowval && nzval)), SMA_ERR_ARG, "null array");
+  rp.assign(n + 1, 0);
+  ci.assign(nnz, 0);
+  require(colptr[0] == index_base && colptr[n] == nnz + index_base, SMA_ERR_ARG,
+          "colptr must start at index_base and end at nnz + index_base");
+  for (int64_t j = 0; j < n; ++j) {
+    const int64_t s = colptr[j] - index_base, e = colptr[j + 1] - index_base;
+    require(s >= 0 && e >= s && e <= nnz, SMA_ERR_ARG, "colptr is not monotone");
+    rp[j] = (int)s;
+    for (int64_t t = s; t < e; ++t) {
+      const int64_t i = rowval[t] - index_base;
+      require(i >= 0 && i < n, SMA_ERR_ARG, "row index out of range");
+      require(t == s || rowval[t] > rowval[t - 1], SMA_ERR_ARG,
+              "row indices must be strictly increasing within each column");
+      ci[t] = (int)i;
+    }
+  }
+  rp[n] = (int)nnz;
+}
+
 int sma_op_create_csc(sma_ctx *ctx, int64_t n, int64_t nnz, const int64_t *colptr,
                       const int64_t *rowval, const double *nzval, int64_t index_base,
                       int64_t check_symmetric, sma_op **out) {
@@ -156,27 +184,8 @@ int sma_op_create_csc(sma_ctx *ctx, int64_t n, int64_t nnz, const int64_t *colpt
     check_ctx(ctx);
     require(out != nullptr, SMA_ERR_ARG, "null output pointer");
     *out = nullptr;
-    require(n >= 0 && nnz >= 0, SMA_ERR_ARG, "negative size");
-    require(n < INT32_MAX && nnz < INT32_MAX, SMA_ERR_ARG, "matrix too large for 32-bit indices");
-    require(index_base == 0 || index_base == 1, SMA_ERR_ARG, "index_base must be 0 or 1");
-    require(colptr != nullptr && (nnz == 0 || (rowval && nzval)), SMA_ERR_ARG, "null array");
-    // Validate on the host so that no device kernel can index out of bounds.
-    std::vector<int> rp(n + 1), ci(nnz);
-    require(colptr[0] == index_base && colptr[n] == nnz + index_base, SMA_ERR_ARG,
-            "colptr must start at index_base and end at nnz + index_base");
-    for (int64_t j = 0; j < n; ++j) {
-      const int64_t s = colptr[j] - index_base, e = colptr[j + 1] - index_base;
-      require(s >= 0 && e >= s && e <= nnz, SMA_ERR_ARG, "colptr is not monotone");
-      rp[j] = (int)s;
-      for (int64_t t = s; t < e; ++t) {
-        const int64_t i = rowval[t] - index_base;
-        require(i >= 0 && i < n, SMA_ERR_ARG, "row index out of range");
-        require(t == s || rowval[t] > rowval[t - 1], SMA_ERR_ARG,
-                "row indices must be strictly increasing within each column");
-        ci[t] = (int)i;
-      }
-    }
-    rp[n] = (int)nnz;
+    std::vector<int> rp, ci;
+    validate_csc(n, nnz, colptr, rowval, nzval, index_base, rp, ci);
     DeviceGuard g(ctx->device);
     auto *op = new sma_op();
     op->ctx = ctx;
@@ -201,6 +210,72 @@ int sma_op_create_csc(sma_ctx *ctx, int64_t n, int64_t nnz, const int64_t *colpt
       if (check_symmetric) {
         op->sym_state = check_csr_device(op) == 0 ? 1 : 2;
         require(op->sym_state == 1, SMA_ERR_NONSYMMETRIC, "matrix is not symmetric");
+      }
+    } catch (...) {
+      free_op(op);
+      throw;
+    }
+    *out = op;
+  });
+}
+
+int sma_op_create_csc_upper(sma_ctx *ctx, int64_t n, int64_t nnz, const int64_t *colptr,
+                            const int64_t *rowval, const double *nzval, int64_t index_base,
+                            int64_t check_symmetric, sma_op **out) {
+  return guarded([&] {
+    check_ctx(ctx);
+    require(out != nullptr, SMA_ERR_ARG, "null output pointer");
+    *out = nullptr;
+    std::vector<int> rp, ci;
+    validate_csc(n, nnz, colptr, rowval, nzval, index_base, rp, ci);
+    // column j of a symmetric CSC is row j: Gershgorin over the full rows, optional exact
+    // symmetry check (a_ij == a_ji for every stored entry), then the upper triangle
+    double gmin = INFINITY, gmax = -INFINITY;
+    std::vector<int> urp(n + 1, 0), uci;
+    std::vector<double> uval;
+    for (int64_t j = 0; j < n; ++j) {
+      double diag = 0.0, off = 0.0;
+      for (int t = rp[j]; t < rp[j + 1]; ++t) {
+        const int i = ci[t];
+        if (i == j) diag = nzval[t]; else off += std::fabs(nzval[t]);
+        if (check_symmetric && i != j) {
+          const int *b = ci.data() + rp[i], *e = ci.data() + rp[i + 1];
+          const int *p = std::lower_bound(b, e, (int)j);
+          require(p != e && *p == (int)j && nzval[p - ci.data()] == nzval[t],
+                  SMA_ERR_NONSYMMETRIC, "matrix is not symmetric");
+        }
+        if (i >= j) {
+          uci.push_back(i);
+          uval.push_back(nzval[t]);
+        }
+      }
+      gmin = std::min(gmin, diag - off);
+      gmax = std::max(gmax, diag + off);
+      urp[j + 1] = (int)uci.size();
+    }
+    const int64_t unnz = (int64_t)uci.size();
+    DeviceGuard g(ctx->device);
+    auto *op = new sma_op();
+    op->ctx = ctx;
+    op->kind = OP_CSR_HALF;
+    op->n = n;
+    op->nnz = unnz;
+    op->sym_state = 1;  // A = U + U^T - D is symmetric by construction
+    try {
+      cudaStream_t st = ctx->stream;
+      SMA_CUDA(cudaMalloc((void **)&op->rowptr, (n + 1) * sizeof(int)));
+      SMA_CUDA(cudaMalloc((void **)&op->colind, std::max<int64_t>(unnz, 1) * sizeof(int)));
+      SMA_CUDA(cudaMalloc((void **)&op->val64, std::max<int64_t>(unnz, 1) * sizeof(double)));
+      SMA_CUDA(cudaMemcpyAsync(op->rowptr, urp.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
+      if (unnz) {
+        SMA_CUDA(cudaMemcpyAsync(op->colind, uci.data(), unnz * sizeof(int), cudaMemcpyHostToDevice, st));
+        SMA_CUDA(cudaMemcpyAsync(op->val64, uval.data(), unnz * sizeof(double), cudaMemcpyHostToDevice, st));
+      }
+      SMA_CUDA(cudaStreamSynchronize(st));
+      if (n > 0) {
+        op->gersh_min = gmin;
+        op->gersh_max = gmax;
+        op->has_gersh = true;
       }
     } catch (...) {
       free_op(op);
@@ -262,7 +337,8 @@ int sma_op_info(const sma_op *op, int64_t *n, int64_t *nnz) {
 int sma_gershgorin_bounds(sma_op *op, double *smin, double *smax) {
   return guarded([&] {
     check_op(op);
-    require(op->kind == OP_CSR, SMA_ERR_ARG, "gershgorin_bounds needs an explicit sparse matrix");
+    require(op->kind == OP_CSR || op->kind == OP_CSR_HALF, SMA_ERR_ARG,
+            "gershgorin_bounds needs an explicit sparse matrix");
     require(op->has_gersh, SMA_ERR_ARG, "empty matrix has no Gershgorin bounds");
     if (smin) *smin = op->gersh_min;
     if (smax) *smax = op->gersh_max;
@@ -332,7 +408,7 @@ int sma_apply_poly_block_dev(sma_op *op, const double *coeffs, int64_t K, double
       SMA_CUDA(cudaStreamSynchronize(st));
     } else {
       require(op->kind != OP_MATBLOCK, SMA_ERR_ARG, "FP32 filtering needs a device operator");
-      if (op->kind == OP_CSR && !op->val32) {
+      if ((op->kind == OP_CSR || op->kind == OP_CSR_HALF) && !op->val32) {
         SMA_CUDA(cudaMalloc((void **)&op->val32, std::max<int64_t>(op->nnz, 1) * sizeof(float)));
         launch_copy_block<double, float>(st, op->nnz, 1, op->val64, 1, op->val32, 1);
       }

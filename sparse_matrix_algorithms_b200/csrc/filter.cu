@@ -29,7 +29,7 @@ void ClenshawWork<T>::ensure(const sma_op *op, int64_t n_, int64_t b, cudaStream
   tmp.alloc(n * b, st);
   q.release();
   y.release();
-  if (op->kind == OP_MATBLOCK) ax.alloc(n * b, st);
+  if (op->kind == OP_MATBLOCK || op->kind == OP_CSR_HALF) ax.alloc(n * b, st);
 }
 
 template <typename T>
@@ -46,7 +46,8 @@ void ClenshawWork<T>::drop_graph() {
 double clenshaw_step_bytes(const sma_op *op, int64_t b, int elem_bytes) {
   // nnz*(value + column index) + row pointers + Q, B1, B2 reads and one write
   double mat = 0.0;
-  if (op->kind == OP_CSR) mat = (double)op->nnz * (elem_bytes + 4) + 4.0 * (op->n + 1);
+  if (op->kind == OP_CSR || op->kind == OP_CSR_HALF)  // half storage: its stored entries
+    mat = (double)op->nnz * (elem_bytes + 4) + 4.0 * (op->n + 1);
   return mat + 4.0 * (double)op->n * (double)b * elem_bytes;
 }
 
@@ -60,12 +61,14 @@ void op_apply(const sma_op *op, cudaStream_t st, const double *X, int64_t ldx, d
     SMA_CUDA(cudaGetLastError());
     return;
   }
+  if (op->kind == OP_CSR_HALF) return half_product<double>(op, st, X, ldx, Y, ldy, b);
   launch_clenshaw_step<double>(op, st, b, nullptr, 0, X, nullptr, ldx, Y, ldy, 0.0, 1.0, 0.0, false);
 }
 
 template <typename T>
 static void matblock_apply(const sma_op *op, cudaStream_t st, const T *X, T *AX, int64_t ld,
                            int64_t b) {
+  if (op->kind == OP_CSR_HALF) return half_product<T>(op, st, X, ld, AX, ld, b);
   if constexpr (sizeof(T) == 8) {
     const int rc = op->fn(op->user, (const double *)X, (double *)AX, op->n, b, ld, (void *)st);
     if (rc != 0) throw Error(SMA_ERR_CALLBACK, "matblock callback returned " + std::to_string(rc));
@@ -99,7 +102,7 @@ static FilterCount record_filter(const sma_op *op, cudaStream_t st,
   const double invd = 2.0 / (smax - smin);
   const double alpha = 2.0 * invd;
   const double beta = -2.0 * c * invd;
-  const bool fused = op->kind != OP_MATBLOCK;
+  const bool fused = op->kind != OP_MATBLOCK && op->kind != OP_CSR_HALF;
   const double blk = (double)n * (double)b * sizeof(T);
   T *B1 = work.b1.p, *B2 = work.b2.p, *TMP = work.tmp.p;
   const int64_t ld = b;
@@ -163,7 +166,8 @@ FilterCount apply_poly_block(const sma_op *op, cudaStream_t st, const std::vecto
     return persistent_filter<T>(op, st, coeffs, smin, smax, Q, ldq, Y, ldy, b, work.b1.p,
                                 work.b2.p, work.tmp.p, work.coef.p, work.barrier.p);
   }
-  if (op->kind == OP_MATBLOCK || K < kGraphMinDegree || !op->ctx->filter_graphs)
+  if (op->kind == OP_MATBLOCK || op->kind == OP_CSR_HALF || K < kGraphMinDegree ||
+      !op->ctx->filter_graphs)
     return record_filter<T>(op, st, coeffs, smin, smax, Q, ldq, Y, ldy, b, work, true);
   // repeated filter -> CUDA graph on the staging blocks
   const bool same = work.g_op == op && work.g_b == b && work.g_smin == smin &&

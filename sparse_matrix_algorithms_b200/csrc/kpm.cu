@@ -62,10 +62,11 @@ void kpm_moments(const sma_op *op, int64_t M, int64_t R, uint64_t seed, double s
   // out = ck Q + alpha A B1 + beta B1: the fused step for device operators, the caller's
   // block product followed by the axpy kernel for callback operators
   DevBuf<double> ax;
-  if (op->kind == OP_MATBLOCK) ax.alloc(n * R, st);
+  const bool product_then_axpy = op->kind == OP_MATBLOCK || op->kind == OP_CSR_HALF;
+  if (product_then_axpy) ax.alloc(n * R, st);
   auto step = [&](const double *Q, const double *B1, double *out, double ck, double alpha,
                   double beta) {
-    if (op->kind == OP_MATBLOCK) {
+    if (product_then_axpy) {
       op_apply(op, st, B1, R, ax.p, R, R);
       launch_clenshaw_axpy<double>(st, n, R, Q, R, ax.p, R, B1, nullptr, R, out, R, ck, alpha, beta);
     } else {

@@ -99,7 +99,8 @@ struct sma_ctx {
   bool persistent = false;
 };
 
-enum op_kind { OP_CSR = 0, OP_LAP1D = 1, OP_MATBLOCK = 2, OP_ANDERSON = 3, OP_XXZ = 4 };
+// OP_CSR_HALF: the upper triangle of a symmetric matrix only (half.cu)
+enum op_kind { OP_CSR = 0, OP_LAP1D = 1, OP_MATBLOCK = 2, OP_ANDERSON = 3, OP_XXZ = 4, OP_CSR_HALF = 5 };
 
 // Data of the matrix-free model stencils (kernels.cu): the 3D Anderson model on an L^3
 // periodic lattice and the XXZ chain in its Sz = 0 sector.
@@ -309,6 +310,11 @@ FilterCount persistent_filter(const sma_op *op, cudaStream_t st, const std::vect
 
 // persistent.cu: the bounded grid barrier with a missing CTA; SMA_ERR_TIMEOUT expected
 int barrier_selftest(sma_ctx *ctx);
+
+// Y = A X for a half-storage operator (row pass + atomic scatter of the transposed half)
+template <typename T>
+void half_product(const sma_op *op, cudaStream_t st, const T *X, int64_t ldx, T *Y, int64_t ldy,
+                  int64_t b);
 
 // AX = A X for FP64 blocks (any operator kind)
 void op_apply(const sma_op *op, cudaStream_t st, const double *X, int64_t ldx, double *Y,

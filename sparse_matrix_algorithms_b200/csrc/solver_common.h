@@ -114,7 +114,7 @@ struct Filter {
 };
 
 inline void ensure_fp32_values(sma_op *op) {
-  if (op->kind != OP_CSR || op->val32) return;
+  if ((op->kind != OP_CSR && op->kind != OP_CSR_HALF) || op->val32) return;
   cudaStream_t st = op->ctx->stream;
   SMA_CUDA(cudaMalloc((void **)&op->val32, std::max<int64_t>(op->nnz, 1) * sizeof(float)));
   launch_copy_block<double, float>(st, op->nnz, 1, op->val64, 1, op->val32, 1);

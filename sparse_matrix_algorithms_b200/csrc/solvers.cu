@@ -172,7 +172,8 @@ sma_result *cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts
   const int64_t degree = o.degree;
   sma_stats stats{};
   if (!mf) {  // chebyshev_subspace_iteration.jl:669-674
-    require(op->kind == OP_CSR, SMA_ERR_ARG, "the sparse overload needs an explicit sparse matrix");
+    require(op->kind == OP_CSR || op->kind == OP_CSR_HALF, SMA_ERR_ARG,
+            "the sparse overload needs an explicit sparse matrix");
     ensure_symmetry_known(op);
     require(op->sym_state == 1, SMA_ERR_NONSYMMETRIC,
             "Chebyshev filtered solver requires a real symmetric matrix");
@@ -188,7 +189,7 @@ sma_result *cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts
   m0 = std::min(m0, n);
   double smin, smax;
   if (!o.has_bounds) {  // chebyshev_subspace_iteration.jl:677-682
-    require(op->kind == OP_CSR && op->has_gersh, SMA_ERR_ARG,
+    require((op->kind == OP_CSR || op->kind == OP_CSR_HALF) && op->has_gersh, SMA_ERR_ARG,
             "gershgorin_bounds needs an explicit sparse matrix: pass smin and smax");
     smin = op->gersh_min;
     smax = op->gersh_max;
