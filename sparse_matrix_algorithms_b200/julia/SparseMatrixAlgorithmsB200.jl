@@ -88,12 +88,15 @@ mutable struct DeviceCSR <: DeviceOperator
     handle::Ptr{Cvoid}
     n::Int
 end
-"Device copy of a symmetric SparseMatrixCSC (its CSC arrays are its CSR arrays)."
-function DeviceCSR(A::SparseMatrixCSC{Float64,Int}; check_symmetric::Bool=false)
+"""Device copy of a symmetric SparseMatrixCSC (its CSC arrays are its CSR arrays);
+`upper=true` keeps only the upper triangle (symmetric half storage: about half the memory,
+slower products)."""
+function DeviceCSR(A::SparseMatrixCSC{Float64,Int}; check_symmetric::Bool=false, upper::Bool=false)
     n = size(A, 1)
     size(A, 2) == n || throw(ArgumentError("A must be square"))
     h = Ref{Ptr{Cvoid}}(C_NULL)
-    check(ccall((:sma_op_create_csc, libsma), Cint,
+    fn = upper ? :sma_op_create_csc_upper : :sma_op_create_csc
+    check(ccall((fn, libsma), Cint,
                 (Ptr{Cvoid}, Int64, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}, Int64, Int64, Ref{Ptr{Cvoid}}),
                 context(), n, nnz(A), A.colptr, A.rowval, A.nzval, 1, check_symmetric, h))
     op = DeviceCSR(h[], n)
