@@ -95,10 +95,15 @@ function DeviceCSR(A::SparseMatrixCSC{Float64,Int}; check_symmetric::Bool=false,
     n = size(A, 1)
     size(A, 2) == n || throw(ArgumentError("A must be square"))
     h = Ref{Ptr{Cvoid}}(C_NULL)
-    fn = upper ? :sma_op_create_csc_upper : :sma_op_create_csc
-    check(ccall((fn, libsma), Cint,
-                (Ptr{Cvoid}, Int64, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}, Int64, Int64, Ref{Ptr{Cvoid}}),
-                context(), n, nnz(A), A.colptr, A.rowval, A.nzval, 1, check_symmetric, h))
+    if upper  # ccall needs the symbol as a constant
+        check(ccall((:sma_op_create_csc_upper, libsma), Cint,
+                    (Ptr{Cvoid}, Int64, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}, Int64, Int64, Ref{Ptr{Cvoid}}),
+                    context(), n, nnz(A), A.colptr, A.rowval, A.nzval, 1, check_symmetric, h))
+    else
+        check(ccall((:sma_op_create_csc, libsma), Cint,
+                    (Ptr{Cvoid}, Int64, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}, Int64, Int64, Ref{Ptr{Cvoid}}),
+                    context(), n, nnz(A), A.colptr, A.rowval, A.nzval, 1, check_symmetric, h))
+    end
     op = DeviceCSR(h[], n)
     finalizer(o -> ccall((:sma_op_destroy, libsma), Cint, (Ptr{Cvoid},), o.handle), op)
     return op
