@@ -1,40 +1,44 @@
-"""Benchmark: eigenpairs/s of POLFED in FP64, chosen configuration vs plain, plus SpMM GB/s.
+"""Benchmark: eigenpairs/s of POLFED on one B200 -- the untuned pipeline against the plain
+FP64 GPU path -- plus the SpMM GB/s of the fused Clenshaw step.
 
-Default workload (one "step" = one full solve) -- the C2 configuration: POLFED in FP64 on
-the random-field XXZ chain L=18, periodic, J=Delta=1, h_i ~ U[-5, 5] (seed 1), Sz=0
-sector (n=48620, ~10.5 nnz/row); the 200 eigenvalues nearest the spectral centre; block
-size s=32, mmax=24.  The window [emin, emax] holds exactly those 200 eigenvalues of the
-dense FP64 spectrum (tests/golden/xxz_L18_spectrum.npz); its ends sit at mid-gaps.
+Default workload (one "step" = one full solve of the window) -- the C3 configuration: the
+3D Anderson model L=64 (n=262144, 7 nnz/row, periodic), W=16.5, seed 2; the 500-eigenvalue
+window centred at E=0 placed by KPM (256 moments, 32 vectors, seed 11) and fixed (it holds
+exactly 494 eigenvalues by Sylvester inertia, tests/golden/anderson_L64_inertia.json);
+block size s=64.  ``--workload c2``: the random-field XXZ chain L=18 (n=48620), h=5, seed
+1; the 200 eigenvalues nearest the spectral centre (exact, from the dense spectrum); s=32.
 
-Two arms per step, both FP64 POLFED through the library:
-  plain   Gershgorin bounds, degree 2200 (the smallest degree of the sweep with which all
-          200 pairs converge);
-  chosen  Lanczos spectral bounds (100 GPU Lanczos steps, INSIDE the timed step), no
-          Jackson damping (the sharper delta filter needs a larger Krylov basis but fewer
-          steps in all), degree 700 and mmax 44: the fewest filter steps of a sweep with
-          which all 200 pairs converge.
-value is the chosen arm; plain_fp64 is the plain arm in the same run; learned_polfed a
-third arm: Lanczos bounds and 256 KPM moments, then the GPU-trained planner's (nev, degree,
-mmax) for the window (Jackson-damped filter, plain-rule fallback), all inside its timed step.
+Arms, all POLFED through the library, the same window:
+  pipeline  (value) nothing tuned for the workload: 100 GPU Lanczos steps for the spectral
+            bounds, 256 KPM moments, then the GPU-trained planner's (nev, degree, mmax)
+            for the window, the plain rule as fallback and judge -- all inside the timed
+            step -- in the arithmetic given by --precision (default: mixed, an FP32 filter
+            basis with FP64 orthogonalization, Rayleigh-Ritz, residuals and polish).
+  plain     the plain FP64 GPU path: Gershgorin bounds, Jackson-damped delta window,
+            degree 12 d / (emax - emin) (C3) or the smallest converging degree of a sweep
+            (C2), mmax = ceil(2.8 nev / s) (polfed.jl:1132).
+  tuned     FP64 with the (window, damping, degree, mmax) that a sweep ON THIS MATRIX found
+            fastest -- reported for reference, not the value.
 
---workload c3: the 3D Anderson model L=64 (n=262144), W=16.5, seed 2; 500 eigenvalues in
-a window centred at E=0 placed by KPM (256 moments, 32 vectors) and fixed; s=64,
-mmax=22, plain degree 12 d / (emax - emin) with the Gershgorin half-width d; chosen: Lanczos
-bounds, no Jackson damping, step window, degree 1200, mmax 44 (the fewest steps of a sweep
-converging all 494 pairs).
-
-value     eigenpairs with relative residual ||Ax-lam x||/||A|| <= 1e-10 found inside the
-          window, per second of device time (CUDA events on the library's stream),
-          matrix resident in HBM; L2 flushed (256 MiB write) before every solve.
-e2e       the chosen arm through the public API with host buffers: CSR upload, bounds,
-          solve, eigenvector download inside the timed region.
-roofline  the fused Clenshaw-SpMM step: algorithmic bytes of all filter launches
-          (12 nnz + 4(n+1) + 32 n b per step, FP64) / device time of the filter phases,
-          against the measured HBM copy bandwidth.
-With --gpus N under torchrun every rank runs an independent replica (the path has no
-data exchange); value is the sum over ranks, timed as the max over ranks.
---impl reference times the CPU restatement of the reference algorithm (oracle/) on a
-bounded sample of the plain arm on all host cores.
+value      eigenpairs inside the window with relative residual ||Ax-lam x||/||A|| <= 1e-10,
+           per second of device time (CUDA events on the library's stream); the matrix is
+           resident in HBM, eigenvectors stay on the device; L2 flushed (256 MiB write)
+           before every solve.  `steps` solves timed after `warmup` untimed ones; the plain
+           and tuned arms run --arm-steps timed solves after one warm-up each.
+e2e        the pipeline through the public API with host buffers: CSR upload, bounds, KPM,
+           plan, solve and eigenvector download inside the timed region (host clock,
+           device synchronized).
+roofline   the fused Clenshaw-SpMM step of the pipeline's filter: algorithmic bytes of all
+           its launches (nnz (s_v + 4) + 4 (n+1) + 4 n b s_x per step) over the device time
+           of the filter phases, against the measured HBM copy bandwidth.
+cpu_baseline  the plain arm's POLFED configuration run by the CPU restatement of the
+           reference (oracle/, FP64, OpenMP over the block's columns, all host threads) on a
+           bounded sample: every block column, a truncated recurrence (its time scaled by
+           degree / steps run), one mid-run reorthogonalization + QR (times mmax), and the
+           extraction (timed, matrix products scaled by the rows run).
+With --gpus N under torchrun every rank runs an independent replica (the path has no data
+exchange); value is the sum over ranks, timed as the max over ranks.
+--impl reference prints the same CPU-restatement measurement as its own line.
 """
 from __future__ import annotations
 
@@ -54,19 +58,15 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "eigenpairs/s at residual<=1e-10: chosen vs plain FP64 on one B200; SpMM GB/s"
-WINDOW = "delta"
 LANCZOS_STEPS = 100
-# dram__bytes_read.sum + dram__bytes_write.sum of one fused Clenshaw step of the C2
-# workload (ncu --set full of one launch of `bench.py --profile-filter --degree 60`)
-TRAFFIC_BYTES_PER_STEP_C2 = 43_698_688 + 242_944
 # the C3 window: 500 eigenvalues by the KPM estimate (256 moments, 32 Rademacher vectors,
 # seed 11, Gershgorin bounds) centred at E=0, fixed here
 C3_WINDOW = (-0.016975627263859053, 0.016979915488252416)
 
 
 def host_gershgorin(A):
-    """Gershgorin interval of a sparse symmetric matrix, on the host (the benchmark's plain
-    degree must not depend on a GPU, since the CPU reference arm builds the same workload)."""
+    """Gershgorin interval of a sparse symmetric matrix, on the host (the plain degree must
+    not depend on a GPU, since the CPU reference arm builds the same workload)."""
     import scipy.sparse as sp
 
     A = sp.csr_matrix(A)
@@ -75,8 +75,16 @@ def host_gershgorin(A):
     return float(np.min(d - r)), float(np.max(d + r))
 
 
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 class Workload:
-    """Matrix, window, POLFED sizes and the plain degree of one benchmark configuration."""
+    """Matrix, window, POLFED sizes and the plain and tuned configurations of one
+    benchmark workload."""
 
     def __init__(self, name):
         from sparse_matrix_algorithms_b200 import matrices as M
@@ -93,67 +101,108 @@ class Workload:
             lo, hi = int(order.min()), int(order.max())
             self.emin = 0.5 * (central[lo - 1] + central[lo])
             self.emax = 0.5 * (central[hi] + central[hi + 1])
+            self.exact = central[lo:hi + 1]
             self.exact_count = hi - lo + 1
             self.norm = max(abs(lam_min), abs(lam_max))
             self.norm_kind = "dense FP64 spectrum"
             # the smallest degree of the sweep {600..2200} x mmax {14, 18, 24} with which
             # every pair reaches residual <= 1e-10 ||A|| (the reference's rule: raise the
             # degree until converged, chebyshev_subspace_iteration.jl:1051)
+            self.window_plain = "delta"
             self.degree_plain = 2200
-            # chosen arm: Lanczos bounds, no Jackson damping; the sweep (degree, mmax) in
-            # {700..1781} x {24..44} (1781/24 with damping) -- the fewest filter steps with
-            # which all 200 pairs converge
-            self.chosen = dict(degree=700, mmax=44, jackson=False, window="delta")
-            self.cpu_columns = 8
-            self.traffic = TRAFFIC_BYTES_PER_STEP_C2
-            self.text = ("C2 POLFED FP64: XXZ L=18 Sz=0 periodic (n=48620), J=Delta=1, "
-                         "h~U[-5,5] seed 1; 200 eigenvalues nearest the spectral centre; s=32")
+            # Lanczos bounds, no Jackson damping; the sweep (degree, mmax) in
+            # {700..1781} x {24..44}: the fewest filter steps with which all 200 converge
+            self.tuned = dict(degree=700, mmax=44, jackson=False, window="delta")
+            self.cpu_steps = 300
+            self.text = ("C2 POLFED: XXZ L=18 Sz=0 periodic (n=48620), J=Delta=1, h~U[-5,5] "
+                         "seed 1; 200 eigenvalues nearest the spectral centre; s=32")
         elif name == "c3":
             self.A = M.config_matrix("anderson_L64")
             self.nev, self.s, self.mmax = 500, 64, 22
             self.emin, self.emax = C3_WINDOW
             # exact count by Sylvester inertia at the two window ends
             # (tests/golden/make_inertia_counts.py -> anderson_L64_inertia.json)
-            gold = os.path.join(ROOT, "tests", "golden", "anderson_L64_inertia.json")
-            self.exact_count = None
-            if os.path.exists(gold):
-                below = json.load(open(gold))
-                self.exact_count = below[repr(self.emax)] - below[repr(self.emin)]
+            below = json.load(open(os.path.join(ROOT, "tests", "golden", "anderson_L64_inertia.json")))
+            self.exact = None
+            self.exact_count = below[repr(self.emax)] - below[repr(self.emin)]
             self.norm = None  # from the Lanczos bounds at set-up
             self.norm_kind = "Lanczos estimate"
             gl, gh = host_gershgorin(self.A)
+            self.window_plain = "delta"
             self.degree_plain = int(12 * 0.5 * (gh - gl) / (self.emax - self.emin))
-            # chosen arm: Lanczos bounds, no Jackson damping; sweep of (window, degree, mmax)
-            # over delta/step x {1200..3857} x {22..50}: the fewest filter steps converging
-            # all 494 pairs (step window 1200/44; the best delta point was 1600/44)
-            self.chosen = dict(degree=1200, mmax=44, jackson=False, window="step")
-            self.cpu_columns = 1
-            # dram__bytes_read.sum + dram__bytes_write.sum of one b=64 FP64 step (ncu --set
-            # full of one launch of `bench.py --profile-filter --workload c3 --width 64`)
-            self.traffic = 429_926_656 + 117_963_264
-            self.text = ("C3 POLFED FP64: 3D Anderson L=64 (n=262144), W=16.5, seed 2, periodic; "
-                         "500 eigenvalues (KPM-placed window centred at E=0); s=64")
+            # Lanczos bounds, no Jackson damping; sweep of (window, degree, mmax) over
+            # delta/step x {1200..3857} x {22..50}: the fewest filter steps converging all
+            # 494 pairs (step window 1200/44; the best delta point was 1600/44)
+            self.tuned = dict(degree=1200, mmax=44, jackson=False, window="step")
+            self.cpu_steps = 120
+            self.text = ("C3 POLFED: 3D Anderson L=64 (n=262144), W=16.5, seed 2, periodic; "
+                         "500 eigenvalues (KPM-placed window centred at E=0, 494 by inertia); s=64")
         else:
             raise ValueError(name)
         self.sigma = 0.5 * (self.emin + self.emax)
 
     def kwargs(self, smin, smax):
         return dict(s=self.s, smin=smin, smax=smax, sigma=self.sigma, emin=self.emin,
-                    emax=self.emax, tol=1e-10, window_type=WINDOW, mmax=self.mmax)
+                    emax=self.emax, tol=1e-10, window_type=self.window_plain, mmax=self.mmax)
 
     def good_pairs(self, lam, res):
         inside = (lam >= self.emin) & (lam <= self.emax)
         return int(np.count_nonzero(inside & (res <= 1e-10 * self.norm)))
 
-    def config(self):
-        return {"workload": self.text, "window_plain": WINDOW, "mmax_plain": self.mmax,
-                "degree_plain": self.degree_plain, "bounds_plain": "Gershgorin",
-                "jackson_plain": True, "degree_chosen": self.chosen["degree"],
-                "mmax_chosen": self.chosen["mmax"], "jackson_chosen": self.chosen["jackson"],
-                "window_chosen": self.chosen["window"],
-                "bounds_chosen": f"Lanczos ({LANCZOS_STEPS} steps, in the timed step)",
+    def config(self, precision):
+        return {"workload": self.text, "window": [self.emin, self.emax],
                 "exact_count_in_window": self.exact_count, "norm": self.norm_kind,
+                "pipeline": {"bounds": f"Lanczos ({LANCZOS_STEPS} steps)", "kpm": "256 moments, 16 vectors",
+                             "plan": "GPU-trained POLFED planner, plain-rule fallback",
+                             "precision": precision, "inside_timed_step": True},
+                "plain": {"bounds": "Gershgorin", "window": self.window_plain, "jackson": True,
+                          "degree": self.degree_plain, "mmax": self.mmax, "precision": "fp64"},
+                "tuned": {"bounds": f"Lanczos ({LANCZOS_STEPS} steps)", **self.tuned,
+                          "precision": "fp64"},
                 "l2": "flushed before every solve (256 MiB write)", "parallelism": "replicas"}
+
+
+# ---------------------------------------------------------------------- the arms
+def arm_plain(wl, op, stats=None, vectors=False):
+    """The plain FP64 GPU path: Gershgorin bounds, plain degree and mmax."""
+    import sparse_matrix_algorithms_b200 as S
+
+    gl, gh = op.gershgorin_bounds()
+    if stats is not None:
+        stats["plan"] = [wl.nev, wl.degree_plain, wl.mmax]
+    return S.polfed(op, wl.nev, wl.degree_plain, stats=stats, vectors=vectors, **wl.kwargs(gl, gh))
+
+
+def arm_tuned(wl, op, stats=None, vectors=False):
+    """FP64 with the sweep-tuned configuration of this workload (Lanczos bounds inside)."""
+    import sparse_matrix_algorithms_b200 as S
+
+    lo, hi = S.lanczos_bounds(op, steps=LANCZOS_STEPS)
+    kw = wl.kwargs(lo, hi)
+    kw.update(mmax=wl.tuned["mmax"], jackson=wl.tuned["jackson"], window_type=wl.tuned["window"])
+    if stats is not None:
+        stats["plan"] = [wl.nev, wl.tuned["degree"], wl.tuned["mmax"]]
+    return S.polfed(op, wl.nev, wl.tuned["degree"], stats=stats, vectors=vectors, **kw)
+
+
+def arm_pipeline(wl, op, net, precision="mixed", stats=None, report=None, vectors=False):
+    """The untuned pipeline: Lanczos bounds, KPM moments, the learned plan with the plain
+    rule as fallback, in the given filter arithmetic."""
+    import sparse_matrix_algorithms_b200 as S
+    from sparse_matrix_algorithms_b200 import planner as P
+
+    lo, hi = S.lanczos_bounds(op, steps=LANCZOS_STEPS)
+    mu = S.kpm_moments(op, P.N_MOMENTS, 16, smin=lo, smax=hi)
+    rep = {}
+    out = P.solve_polfed_window(op, (wl.emin, wl.emax), net, s=wl.s, smin=lo, smax=hi, mu=mu,
+                                report=rep, stats=stats, precision=precision, vectors=vectors)
+    if stats is not None:
+        stats["plan"] = list(rep["plan"])
+        stats["plain_rule"] = list(rep["plain"])
+        stats["redone"] = rep["redone"]
+    if report is not None:
+        report.update(rep)
+    return out
 
 
 class ClockSampler:
@@ -166,7 +215,6 @@ class ClockSampler:
 
     def __enter__(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), "--query-gpu=index,clocks.sm,clocks.max.sm,"
@@ -209,45 +257,91 @@ def measured_hbm_peak():
     return 6650.0, "fallback"
 
 
-def cpu_sample(wl: Workload, threads: int, max_degree: int = 0):
-    """Oracle (CPU restatement) estimate of one plain-arm POLFED block, in seconds: the
-    Clenshaw filter timed on ``wl.cpu_columns`` of the block's s columns (each column's
-    recurrence is independent, identical work) and scaled to the block -- and, when
-    ``max_degree`` truncates the recurrence, scaled from the steps run to the full degree
-    -- plus the timed reorthogonalization and QR of a full mid-run block, on all host
-    cores.  A solve is mmax such blocks; the extraction is not counted (it favours the
-    CPU)."""
+# ---------------------------------------------------------------------- CPU baseline
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import sma_oracle as O
+
+    return O
+
+
+def cpu_plain_estimate(wl: Workload, threads: int) -> dict:
+    """Seconds of one plain-arm POLFED solve by the CPU restatement (oracle, FP64), from a
+    bounded sample on ``threads`` host threads:
+
+    * filter: every one of the block's s columns through a recurrence truncated to
+      ``wl.cpu_steps`` sparse products, timed and scaled by degree / cpu_steps (every step
+      of the recurrence is the same work), times mmax blocks;
+    * block dense work: the reorthogonalization of a block against a mid-run basis of
+      mmax s / 2 columns and its rank-revealing QR, timed, times mmax;
+    * extraction: eigen of the (mmax s)^2 projected matrix, timed in full; the Ritz-vector
+      lift V U and the Rayleigh quotients (one sparse product) over the 2 nev candidates,
+      timed on n / 16 rows and m / 8 columns and scaled; the refinement counted as a
+      second Rayleigh pass.
+    """
+    O = _oracle()
     from sparse_matrix_algorithms_b200 import matrices as M
 
     A = wl.A
-    n = A.shape[0]
+    n, s, mmax = A.shape[0], wl.s, wl.mmax
     smin, smax = O.gershgorin_bounds(A)
-    K = wl.degree_plain if not max_degree else min(max_degree, wl.degree_plain)
-    coeffs = O.build_coeffs(K, smin, smax, wl.sigma, wl.emin, wl.emax, WINDOW, True)
-    Q = O.orth_block(M.splitmix_normal(1, n, wl.s))
-    V = np.linalg.qr(M.splitmix_normal(2, n, wl.s * wl.mmax // 2))[0]
+    D = min(wl.cpu_steps, wl.degree_plain)
+    coeffs = O.build_coeffs(D, smin, smax, wl.sigma, wl.emin, wl.emax, wl.window_plain, True)
+    Q = O.orth_block(M.splitmix_normal(1, n, s))
     t0 = time.perf_counter()
-    O.apply_poly_block(A, Q[:, :wl.cpu_columns], coeffs, smin, smax, impl="c", nthreads=threads)
-    t_filter = (time.perf_counter() - t0) * (wl.s / wl.cpu_columns) * (wl.degree_plain / K)
+    O.apply_poly_block(A, Q, coeffs, smin, smax, impl="c", nthreads=threads)
+    t_filter = (time.perf_counter() - t0) * wl.degree_plain / D
+    V = np.linalg.qr(M.splitmix_normal(2, n, s * mmax // 2))[0]
     W = Q.copy()
     t1 = time.perf_counter()
-    W -= V @ (V.T @ W)  # the reorthogonalization of a mid-run block
+    W -= V @ (V.T @ W)
     O.block_qr_factor(W)
-    return t_filter + (time.perf_counter() - t1)
+    t_block = time.perf_counter() - t1
+    Mdim = s * mmax
+    m = min(Mdim, max(2 * wl.nev, wl.nev + 8))
+    rng = np.random.default_rng(0)
+    T = rng.standard_normal((Mdim, Mdim))
+    T = T + T.T
+    t2 = time.perf_counter()
+    _, U = np.linalg.eigh(T)
+    t_eig = time.perf_counter() - t2
+    rows = max(1, n // 16)
+    Vs = np.ascontiguousarray(rng.standard_normal((rows, Mdim)))
+    t3 = time.perf_counter()
+    Vs @ U[:, :m]
+    t_lift = (time.perf_counter() - t3) * n / rows
+    mc = max(1, m // 8)
+    Xs = np.asfortranarray(rng.standard_normal((n, mc)))
+    t4 = time.perf_counter()
+    O.rayleigh(A, Xs)
+    t_ray = (time.perf_counter() - t4) * m / mc
+    total = mmax * (t_filter + t_block) + t_eig + t_lift + 2 * t_ray
+    return {"seconds": total, "filter_s": mmax * t_filter, "block_dense_s": mmax * t_block,
+            "extract_s": t_eig + t_lift + 2 * t_ray}
 
 
-def _cpu_text(wl: Workload, max_degree: int) -> str:
-    trunc = (f", recurrence truncated to {max_degree} steps and scaled to {wl.degree_plain}"
-             if max_degree and max_degree < wl.degree_plain else "")
-    return (f"one POLFED block of the CPU restatement (oracle/clenshaw_ref.c filter of degree "
-            f"{wl.degree_plain} timed on {wl.cpu_columns} of the {wl.s} columns and scaled{trunc}; "
-            f"the block's reorthogonalization and QR) x {wl.mmax} blocks; extraction not counted; "
-            f"credited with the {wl.nev} pairs the full solve finds")
+def cpu_text(wl: Workload) -> str:
+    return (f"the plain arm's configuration (Gershgorin bounds, Jackson-damped {wl.window_plain} "
+            f"window, degree {wl.degree_plain}, mmax {wl.mmax}, s {wl.s}) in the CPU restatement "
+            f"(oracle/, FP64): all {wl.s} block columns through {min(wl.cpu_steps, wl.degree_plain)} "
+            f"recurrence steps, scaled to the degree, x {wl.mmax} blocks; one mid-run "
+            f"reorthogonalization + QR x {wl.mmax}; extraction timed (products scaled from "
+            f"row / column slices); credited with the exact count {wl.exact_count} in the window")
 
 
-CPU_MAX_DEGREE = {"c2": 0, "c3": 400}
+def cpu_full_solve(wl: Workload, threads: int) -> dict:
+    """One complete plain-arm POLFED solve by the CPU restatement: wall time and the pairs
+    it found inside the window at relative residual <= 1e-10 (the check of the sampled
+    estimate; minutes of host time for C2)."""
+    O = _oracle()
+    smin, smax = O.gershgorin_bounds(wl.A)
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    t0 = time.perf_counter()
+    lam, X, res = O.polfed(wl.A, wl.nev, wl.degree_plain, **wl.kwargs(smin, smax))
+    dt = time.perf_counter() - t0
+    norm = wl.norm if wl.norm is not None else max(abs(smin), abs(smax))
+    good = int(np.sum((lam >= wl.emin) & (lam <= wl.emax) & (res <= 1e-10 * norm)))
+    return {"seconds": dt, "pairs": good, "threads": threads}
 
 
 def reduce_over_ranks(c_ms, p_ms, c_pairs, p_pairs, device=None):
@@ -267,20 +361,26 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     wl = Workload(args.workload)
-    threads = os.cpu_count() or 1
-    md = CPU_MAX_DEGREE[wl.name]
+    threads = host_threads()
+    if args.cpu_full_solve:
+        est = cpu_plain_estimate(wl, threads)
+        full = cpu_full_solve(wl, threads)
+        print(json.dumps({"cpu_full_solve": wl.name, **full, "sampled_estimate_s": est["seconds"],
+                          "estimate_over_full": est["seconds"] / full["seconds"]}), flush=True)
+        return
     for _ in range(args.warmup):
-        cpu_sample(wl, threads, md)
-    t = [cpu_sample(wl, threads, md) for _ in range(args.steps)]
-    t_block = sum(t) / len(t)
-    value = wl.nev / (t_block * wl.mmax)
+        cpu_plain_estimate(wl, threads)
+    t = [cpu_plain_estimate(wl, threads)["seconds"] for _ in range(args.steps)]
+    t_solve = sum(t) / len(t)
+    value = wl.exact_count / t_solve
     line = {
         "metric": METRIC, "impl": "reference", "value": value, "unit": "eigenpairs/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * t_block, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": wl.config(),
+        "ms_per_step": 1e3 * t_solve, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": wl.config(args.precision),
         "cpu_baseline": {"value": value, "unit": "eigenpairs/s", "cores": threads, "kind": "port",
-                         "sample": "per step " + _cpu_text(wl, md)},
+                         "sample": "per step, one estimated solve: " + cpu_text(wl)},
         "e2e": {"value": value, "unit": "eigenpairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -291,54 +391,35 @@ def run_ours(args, rank, world, device):
 
     import sparse_matrix_algorithms_b200 as S
     from sparse_matrix_algorithms_b200 import _lib as L
+    from sparse_matrix_algorithms_b200 import planner as P
 
     wl = Workload(args.workload)
     A = wl.A
     ctx = S.context(device)
     op = S.SparseOperator(A, ctx)
-    gl, gh = op.gershgorin_bounds()
     if wl.norm is None:
         lo, hi = S.lanczos_bounds(op, steps=LANCZOS_STEPS)
         wl.norm = max(abs(lo), abs(hi))
     stream = torch.cuda.ExternalStream(ctx.stream, device=device)
     flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=device)
     lib = L.load()
+    net = P.WindowPlanner.load(P.POLFED_WEIGHTS)
 
-    def plain(stats=None):
-        return S.polfed(op, wl.nev, wl.degree_plain, stats=stats, **wl.kwargs(gl, gh))
+    def pipeline(st):
+        return arm_pipeline(wl, op, net, args.precision, stats=st)
 
-    def chosen(stats=None, operator=None):
-        o = operator or op
-        lo, hi = S.lanczos_bounds(o, steps=LANCZOS_STEPS)
-        kw = wl.kwargs(lo, hi)
-        kw["mmax"] = wl.chosen["mmax"]
-        kw["jackson"] = wl.chosen["jackson"]
-        kw["window_type"] = wl.chosen["window"]
-        if stats is not None:
-            stats["degree"] = wl.chosen["degree"]
-        return S.polfed(o, wl.nev, wl.chosen["degree"], stats=stats, **kw)
+    def plain(st):
+        return arm_plain(wl, op, stats=st)
+
+    def tuned(st):
+        return arm_tuned(wl, op, stats=st)
 
     step_ms = {}
+    plans = {}
 
-    from sparse_matrix_algorithms_b200 import planner as P
-
-    net = P.WindowPlanner.load(P.POLFED_WEIGHTS)
-    plan_seen = {}
-
-    def learned(stats=None):
-        lo, hi = S.lanczos_bounds(op, steps=LANCZOS_STEPS)
-        mu = S.kpm_moments(op, P.N_MOMENTS, 16, smin=lo, smax=hi)
-        rep = {}
-        out = P.solve_polfed_window(op, (wl.emin, wl.emax), net, s=wl.s, smin=lo, smax=hi, mu=mu,
-                                    report=rep, stats=stats)
-        plan_seen.update(plan=list(rep["plan"]), plain_rule=list(rep["plain"]),
-                         redone=rep["redone"])
-        return out
-
-    def timed(fn, steps):
+    def timed(name, fn, steps):
         pairs, ms, launches = 0, [], 0
-        agg = {"filter_bytes": 0.0, "filter_ms": 0.0}
-        degree = None
+        agg = {"filter_bytes": 0.0, "filter_ms": 0.0, "orth_ms": 0.0, "rr_ms": 0.0}
         for _ in range(steps):
             flush.zero_()
             torch.cuda.synchronize(device)
@@ -346,7 +427,7 @@ def run_ours(args, rank, world, device):
             l0 = lib.sma_kernel_launch_count()
             e0.record(stream)
             st = {}
-            lam, X, res = fn(st)
+            lam, _, res = fn(st)
             e1.record(stream)
             e1.synchronize()
             launches += lib.sma_kernel_launch_count() - l0
@@ -354,41 +435,45 @@ def run_ours(args, rank, world, device):
             pairs += wl.good_pairs(lam, res)
             for k in agg:
                 agg[k] += st[k]
-            degree = st.get("degree")
-        step_ms.setdefault(fn.__name__, []).extend(round(m, 1) for m in ms)
-        return pairs, sum(ms), agg, launches, degree
+            plans[name] = {k: st[k] for k in ("plan", "plain_rule", "redone", "polish_iterations",
+                                              "fp32_filter_calls", "basis_dim") if k in st}
+        step_ms[name] = [round(m, 1) for m in ms]
+        return pairs, sum(ms), agg, launches
 
+    arm_steps = max(1, min(args.arm_steps, args.steps))
     # the clock sampler starts before the warm-up: starting nvidia-smi stalls the GPU's
     # work for about a second, which must not fall into a timed solve
     with ClockSampler(device) as clk:
         for _ in range(args.warmup):
-            plain()
-            chosen()
-            learned()
+            pipeline({})
+        plain({})
+        tuned({})
         torch.cuda.synchronize(device)
         if world > 1:
             torch.distributed.barrier()
-        c_pairs, c_ms, c_agg, c_launch, _ = timed(chosen, args.steps)
+        v_pairs, v_ms, v_agg, v_launch = timed("pipeline", pipeline, args.steps)
         torch.cuda.synchronize(device)
-        p_pairs, p_ms, p_agg, _, _ = timed(plain, args.steps)
-        l_pairs, l_ms, _, _, _ = timed(learned, args.steps)
+        p_pairs, p_ms, p_agg, _ = timed("plain", plain, arm_steps)
+        t_pairs, t_ms, _, _ = timed("tuned", tuned, arm_steps)
     if world > 1:
-        c_ms, p_ms, c_pairs, p_pairs = reduce_over_ranks(c_ms, p_ms, c_pairs, p_pairs, device)
-        l_ms, _, l_pairs, _ = reduce_over_ranks(l_ms, 0.0, l_pairs, 0, device)
-    value = c_pairs / (c_ms / 1e3)
+        v_ms, p_ms, v_pairs, p_pairs = reduce_over_ranks(v_ms, p_ms, v_pairs, p_pairs, device)
+        t_ms, _, t_pairs, _ = reduce_over_ranks(t_ms, 0.0, t_pairs, 0, device)
+    value = v_pairs / (v_ms / 1e3)
     plain_value = p_pairs / (p_ms / 1e3)
+    tuned_value = t_pairs / (t_ms / 1e3)
 
-    # end to end through the public API with host buffers: upload, bounds, solve, download
+    # end to end through the public API with host buffers: upload, bounds, KPM, plan,
+    # solve, eigenvector download
     e2e_ms, e2e_pairs = [], 0
     h2d = 8 * (A.shape[0] + 1) + 16 * A.nnz
     d2h = 0
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = max(1, min(args.steps, 2))
     for _ in range(e2e_steps):
         flush.zero_()
         torch.cuda.synchronize(device)
         t0 = time.perf_counter()
         hop = S.SparseOperator(A, ctx)
-        lam, X, res = chosen(None, hop)
+        lam, X, res = arm_pipeline(wl, hop, net, args.precision, vectors=True)
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
         e2e_pairs += wl.good_pairs(lam, res)
         d2h = 8 * (X.size + lam.size + res.size)
@@ -400,47 +485,55 @@ def run_ours(args, rank, world, device):
     if rank != 0:
         return
     peak, peak_kind = measured_hbm_peak()
-    achieved = c_agg["filter_bytes"] / (c_agg["filter_ms"] / 1e3) / 1e9
+    achieved = v_agg["filter_bytes"] / (v_agg["filter_ms"] / 1e3) / 1e9
     cpu = None
-    if world == 1:
-        threads = os.cpu_count() or 1
-        md = CPU_MAX_DEGREE[wl.name]
-        t_block = cpu_sample(wl, threads, md)
-        cpu = {"value": wl.nev / (t_block * wl.mmax), "unit": "eigenpairs/s", "cores": threads,
-               "kind": "port", "sample": _cpu_text(wl, md)}
-    cfg = wl.config()
+    if world == 1 and not args.no_cpu:
+        threads = host_threads()
+        est = cpu_plain_estimate(wl, threads)
+        cpu_value = min(wl.exact_count, p_pairs / arm_steps) / est["seconds"]
+        cpu = {"value": cpu_value, "unit": "eigenpairs/s", "cores": threads, "kind": "port",
+               "sample": cpu_text(wl), "seconds_per_solve": est["seconds"],
+               "gpu_plain_over_cpu_plain": plain_value / cpu_value,
+               "value_over_cpu_plain": value / cpu_value}
+    dtype = {"fp64": "f64", "fp32": "f32", "mixed": "f32 filter + f64 orth/RR/residual/polish"}
     line = {
         "metric": METRIC, "value": value, "unit": "eigenpairs/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": c_ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": cfg,
-        "pairs_per_step": c_pairs / args.steps / world,
-        "plain_fp64": {"value": plain_value, "unit": "eigenpairs/s",
-                       "ms_per_step": p_ms / args.steps,
-                       "pairs_per_step": p_pairs / args.steps / world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": dtype[args.precision], "data": "synthetic", "config": wl.config(args.precision),
+        "pairs_per_step": v_pairs / args.steps / world,
+        "pipeline_over_plain": value / plain_value if plain_value > 0 else None,
+        "plain_fp64": {"value": plain_value, "unit": "eigenpairs/s", "ms_per_step": p_ms / arm_steps,
+                       "pairs_per_step": p_pairs / arm_steps / world,
                        "spmm_gbs": p_agg["filter_bytes"] / (p_agg["filter_ms"] / 1e3) / 1e9},
-        "chosen_vs_plain": value / plain_value if plain_value > 0 else None,
-        "learned_polfed": {"value": l_pairs / (l_ms / 1e3), "unit": "eigenpairs/s",
-                           "ms_per_step": l_ms / args.steps,
-                           "pairs_per_step": l_pairs / args.steps / world,
-                           "vs_plain": (l_pairs / (l_ms / 1e3)) / plain_value if plain_value > 0 else None,
-                           "what": "Lanczos bounds + 256 KPM moments + the GPU-trained planner's "
-                                   "(nev, degree, mmax) for the window, Jackson-damped, plain-rule "
-                                   "fallback; all inside the timed step", **plan_seen},
+        "tuned_fp64": {"value": tuned_value, "unit": "eigenpairs/s", "ms_per_step": t_ms / arm_steps,
+                       "pairs_per_step": t_pairs / arm_steps / world,
+                       "over_plain": tuned_value / plain_value if plain_value > 0 else None},
+        "plans": plans,
+        "phase_ms_per_step": {k: v_agg[k] / args.steps for k in ("filter_ms", "orth_ms", "rr_ms")},
         "step_ms": step_ms,
         "spmm_gbs": achieved,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": wl.traffic,
-                     "kernel": "fused CSR Clenshaw step (SpMM + recurrence axpy)",
+                     "frac": achieved / peak, "traffic": TRAFFIC.get((wl.name, args.precision)),
+                     "kernel": "fused CSR Clenshaw step (SpMM + recurrence axpy), all filter launches",
                      "peak_kind": f"{peak_kind} HBM copy bandwidth",
                      "note": ("working set (~56 MB) is L2-resident at this size"
-                              if wl.name == "c2" else "blocks of 134 MB per step exceed L2")},
+                              if wl.name == "c2" else "blocks of 67-134 MB per step exceed L2")},
         "e2e": e2e,
-        "gpu_launches": c_launch,
+        "gpu_launches": v_launch,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
+
+
+# dram__bytes_read.sum + dram__bytes_write.sum of one fused Clenshaw step of the arm's
+# dominant block shape, per launch (ncu of `bench.py --profile-filter ...`); None when no
+# capture of that shape exists
+TRAFFIC = {
+    ("c2", "fp64"): 43_698_688 + 242_944,
+    ("c3", "fp64"): 429_926_656 + 117_963_264,
+}
 
 
 def run_profile_filter(args):
@@ -460,20 +553,22 @@ def run_profile_filter(args):
     width = args.width or wl.s
     Q = torch.randn(wl.A.shape[0], width, dtype=dt, device="cuda")
     Y = torch.empty_like(Q)
-    c = np.ascontiguousarray(S.build_coeffs(args.degree, smin, smax, wl.sigma, wl.emin, wl.emax, WINDOW))
+    c = np.ascontiguousarray(S.build_coeffs(args.degree, smin, smax, wl.sigma, wl.emin, wl.emax,
+                                            wl.window_plain))
     stream = torch.cuda.ExternalStream(ctx.stream)
     torch.cuda.synchronize()
     times = []
+    prec = "fp64" if args.precision == "fp64" else "fp32"
     for _ in range(args.calls):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         L.check(L.load().sma_apply_poly_block_dev(op.handle, c.ctypes.data, args.degree, smin, smax,
                                                   Q.data_ptr(), width, Y.data_ptr(), width, width,
-                                                  L.PRECISIONS[args.precision]))
+                                                  L.PRECISIONS[prec]))
         e1.record(stream)
         e1.synchronize()
         times.append(e0.elapsed_time(e1) / args.degree)
-    print(json.dumps({"profile_filter": args.precision, "workload": wl.name, "width": width,
+    print(json.dumps({"profile_filter": prec, "workload": wl.name, "width": width,
                       "degree": args.degree, "us_per_step_last": 1e3 * times[-1]}), flush=True)
 
 
@@ -490,7 +585,7 @@ def run_profile_orth(args):
     st = {}
     kw = wl.kwargs(gl, gh)
     kw["mmax"] = 8
-    S.polfed(op, 100, 60, stats=st, **kw)
+    S.polfed(op, 100, 60, stats=st, vectors=False, **kw)
     print(json.dumps({"profile_orth": "c3", "orth_ms": st["orth_ms"], "rr_ms": st["rr_ms"],
                       "filter_ms": st["filter_ms"], "basis_dim": st["basis_dim"]}), flush=True)
 
@@ -517,15 +612,21 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--arm-steps", type=int, default=2,
+                    help="timed solves of the plain and tuned arms (each after one warm-up)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3"])
+    ap.add_argument("--workload", default="c3", choices=["c2", "c3"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "fp32", "mixed"],
+                    help="filter arithmetic of the pipeline arm (and of --profile-filter)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--cpu-full-solve", action="store_true",
+                    help="with --impl reference: one complete CPU solve plus the sampled estimate")
     ap.add_argument("--profile-filter", action="store_true",
                     help="run only the Clenshaw filter of the workload (for ncu captures)")
     ap.add_argument("--profile-orth", action="store_true",
                     help="a short C3 POLFED solve for ncu captures of its GEMMs")
     ap.add_argument("--profile-slice", action="store_true",
                     help="one batched slicing iteration on the C3 matrix for ncu captures")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--width", type=int, default=0, help="block width (default: the workload's s)")
     ap.add_argument("--degree", type=int, default=60)
     ap.add_argument("--calls", type=int, default=3)

@@ -184,8 +184,10 @@ int sma_op_create_csc(sma_ctx *ctx, int64_t n, int64_t nnz, const int64_t *colpt
  * (diagonal included) is kept on the device, about half the entries and indices.  Products
  * are a row pass plus an atomic scatter of the transposed half, so they agree with full
  * storage to rounding, not bit for bit; the filter runs as product + axpy.  The lower
- * triangle is not stored: with check_symmetric != 0 the host verifies a_ij == a_ji first.
- * Gershgorin bounds come from the full rows.  Not accepted by sma_slice_solve. */
+ * triangle is ignored: the operator applied is U + U^T - D for the stored upper triangle
+ * U (diagonal D), whatever the lower triangle held; check_symmetric != 0 verifies
+ * a_ij == a_ji on the host first and rejects a non-symmetric input.  Gershgorin bounds are
+ * those of the operator applied.  Not accepted by sma_slice_solve. */
 int sma_op_create_csc_upper(sma_ctx *ctx, int64_t n, int64_t nnz, const int64_t *colptr,
                             const int64_t *rowval, const double *nzval, int64_t index_base,
                             int64_t check_symmetric, sma_op **out);
@@ -258,6 +260,36 @@ int sma_apply_poly_block_dev(sma_op *op, const double *coeffs, int64_t K, double
 int sma_apply_poly_block(sma_op *op, const double *coeffs, int64_t K, double smin,
                          double smax, const double *Q, double *Y, int64_t b,
                          int64_t precision);
+/* The block filter with one polynomial per column (an extension; the reference filters a
+ * block with one polynomial): column j of Y_dev is sum_m coeffs[m*b + j] T_m(A_hat) applied
+ * to column j of Q_dev, by the same Clenshaw recurrence, for row-major n x b device blocks
+ * with leading dimension b.  coeffs: (K+1) x b host doubles, row-major.  precision as in
+ * sma_apply_poly_block_dev.  On a CSR matrix each column is bit-identical to
+ * sma_apply_poly_block_dev with that column's coefficients.  Device operators only.
+ * MIXED-precision POLFED uses it to apply, per Ritz vector, the divided difference of its
+ * filter in FP32.  Synchronous. */
+int sma_apply_poly_block_percol_dev(sma_op *op, const double *coeffs, int64_t K, double smin,
+                                    double smax, const void *Q_dev, void *Y_dev, int64_t b,
+                                    int64_t precision);
+/* Divided difference of p = sum_{m=0..K} coeffs[m] T_m at t (K >= 1): e[0..K-1] with
+ * (p(s) - p(t)) / (s - t) = sum_m e[m] T_m(s), and *pt = p(t) (an extension used by the
+ * MIXED POLFED polish). */
+int sma_divided_difference(const double *coeffs, int64_t K, double t, double *e, double *pt);
+/* The tall-skinny FP64 products of the block orthogonalization and Rayleigh-Ritz steps
+ * (the reference's Q' W and W - Q C of orth_against!/reorth_full!, polfed.jl:605-631, and
+ * X = Q Xq of chebyshev_subspace_iteration.jl:735-740), on this library's FP64 tensor-core
+ * (DMMA) kernels, exposed for callers and tests:
+ *   gram:   C (m x k, column-major, ldc) = alpha X^T Y + beta C, X n x m and Y n x k
+ *           row-major device blocks; deterministic (split-n partials summed in order);
+ *   update: Y (n x p, row-major) = alpha X B + beta Y, X n x m row-major, B = C (m x p,
+ *           column-major, ldc) or, with transC != 0, B = C^T (C p x m column-major).
+ * Device pointers; synchronous. */
+int sma_dense_gram_dev(sma_ctx *ctx, int64_t n, int64_t m, int64_t k, const double *X_dev,
+                       int64_t ldx, const double *Y_dev, int64_t ldy, double *C_dev, int64_t ldc,
+                       double alpha, double beta);
+int sma_dense_update_dev(sma_ctx *ctx, int64_t n, int64_t m, int64_t p, const double *X_dev,
+                         int64_t ldx, const double *C_dev, int64_t ldc, int64_t transC,
+                         double *Y_dev, int64_t ldy, double alpha, double beta);
 /* Y = A X on device row-major FP64 blocks (apply_A_block!). Synchronous. */
 int sma_spmm_dev(sma_op *op, const double *X_dev, int64_t ldx, double *Y_dev, int64_t ldy,
                  int64_t b);
@@ -267,7 +299,8 @@ int sma_spmm_dev(sma_op *op, const double *X_dev, int64_t ldx, double *Y_dev, in
  * No counterpart in the reference (its filter allocates Julia arrays).  Its three n x b
  * recurrence blocks live in one static device array of 48 MiB (held on every device that
  * loads it until exit), so n*b must be <= 2,097,152 (else SMA_ERR_ARG).  Device operators
- * only (CSR or stencil).  All calls on a device share the array: calls that overlap on
+ * only: CSR or a model stencil (1D Laplacian, Anderson, XXZ); half storage and caller
+ * callbacks are rejected.  All calls on a device share the array: calls that overlap on
  * the GPU race, so serialize them.  The first call on a device looks the array up; make
  * it before any stream capture.  Synchronous. */
 int sma_apply_poly_block_noalloc(sma_op *op, const double *coeffs, int64_t K, double smin,
@@ -285,6 +318,26 @@ int sma_cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts *op
  * smallest residual is below tol, else by residual). */
 int sma_polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polfed_opts *opts,
                      sma_result **out);
+
+/* Batched POLFED (no counterpart in the reference, which runs polfed on one window per call,
+ * polfed.jl:1128): nwin windows [emin[w], emax[w]] over the same explicit sparse matrix, each
+ * a POLFED solve with its own nev[w], filter degree[w] and basis size mmax[w] blocks, its
+ * filter centred on the window (sigma = (emin[w] + emax[w]) / 2) and start block seed
+ * opts->seed + w.  The other options (s, smin, smax, tol, window_type, jackson, precision,
+ * overextract, refine, rtol, reorth_passes, extra_keep, show_progress) apply to every
+ * window; opts->emin/emax/sigma/mmax are ignored.  Every block step filters all active
+ * windows' blocks in ONE segmented Clenshaw recurrence (windows sorted by degree, each
+ * column with its own window's coefficients, recorded into a CUDA graph and replayed), so
+ * each window's filtered block is bit-identical to its single-window filter and the matrix
+ * is read once per step for all windows; a window leaves the batch when its basis is
+ * complete.  MIXED: the basis filter in FP32, each window's pairs polished to FP64 accuracy.
+ * The result holds window 0's pairs (in polfed's return order), then window 1's, ...;
+ * sma_result_windows gives the window of every pair, sma_result_window_info each window's
+ * blocks and whether the return rule's by-eigenvalue branch applied (the nev-th residual
+ * below tol). */
+int sma_polfed_batch_solve(sma_op *op, int64_t nwin, const double *emin, const double *emax,
+                           const int64_t *nev, const int64_t *degree, const int64_t *mmax,
+                           const sma_polfed_opts *opts, sma_result **out);
 
 /* Batched spectrum slicing (no counterpart in the reference, which solves one window per
  * call): nwin windows [emin[w], emax[w]] over the same operator, each with its own filter

@@ -641,3 +641,21 @@ def kpm_count(mu, n: int, smin: float, smax: float, emin: float, emax: float,
     s = g[0] * mu[0] * (ta - tb) + np.sum(2.0 * g[1:] * np.asarray(mu[1:]) *
                                           (np.sin(k * ta) - np.sin(k * tb)) / k)
     return float(n * s / math.pi)
+
+
+def divided_difference(c, t: float):
+    """Chebyshev coefficients e of (p(s) - p(t)) / (s - t) for p = sum c_m T_m, and p(t).
+
+    No counterpart in the reference (it is the FP32 polish of this library's MIXED POLFED).
+    Computed here by numpy's Chebyshev-series long division of p - p(t) by (s - t), a route
+    independent of the library's (the Clenshaw intermediates of p at t)."""
+    from numpy.polynomial import chebyshev as C
+
+    c = np.asarray(c, dtype=np.float64)
+    pt = float(C.chebval(t, c))
+    num = c.copy()
+    num[0] -= pt
+    q, _ = C.chebdiv(num, np.array([-t, 1.0]))
+    e = np.zeros(len(c) - 1)
+    e[:len(q)] = q
+    return e, pt

@@ -29,6 +29,7 @@ from .api import (  # noqa: F401
     kpm_moments,
     lanczos_bounds,
     polfed,
+    polfed_windows,
     slice_spectrum,
 )
 from . import matrices  # noqa: F401

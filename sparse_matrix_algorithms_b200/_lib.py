@@ -134,6 +134,14 @@ SIGNATURES = [
     ("sma_apply_poly_block", c_int, [c_void_p, c_void_p, c_int64, c_double, c_double, c_void_p,
                                      c_void_p, c_int64, c_int64]),
     ("sma_spmm_dev", c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int64, c_int64]),
+    ("sma_apply_poly_block_percol_dev", c_int, [c_void_p, c_void_p, c_int64, c_double, c_double,
+                                                c_void_p, c_void_p, c_int64, c_int64]),
+    ("sma_dense_gram_dev", c_int, [c_void_p, c_int64, c_int64, c_int64, c_void_p, c_int64,
+                                   c_void_p, c_int64, c_void_p, c_int64, c_double, c_double]),
+    ("sma_dense_update_dev", c_int, [c_void_p, c_int64, c_int64, c_int64, c_void_p, c_int64,
+                                     c_void_p, c_int64, c_int64, c_void_p, c_int64, c_double,
+                                     c_double]),
+    ("sma_divided_difference", c_int, [c_void_p, c_int64, c_double, c_void_p, c_void_p]),
     ("sma_apply_poly_block_noalloc", c_int, [c_void_p, c_void_p, c_int64, c_double, c_double,
                                              c_void_p, c_int64, c_void_p, c_int64, c_int64]),
     ("sma_kpm_moments", c_int, [c_void_p, c_int64, c_int64, c_int64, c_double, c_double,
@@ -146,6 +154,8 @@ SIGNATURES = [
                                ctypes.POINTER(c_void_p)]),
     ("sma_polfed_solve", c_int, [c_void_p, c_int64, c_int64, ctypes.POINTER(PolfedOpts),
                                  ctypes.POINTER(c_void_p)]),
+    ("sma_polfed_batch_solve", c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p,
+                                       c_void_p, c_void_p, c_void_p, ctypes.POINTER(c_void_p)]),
     ("sma_slice_opts_default", None, [ctypes.POINTER(SliceOpts)]),
     ("sma_slice_solve", c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p,
                                 ctypes.POINTER(SliceOpts), ctypes.POINTER(c_void_p)]),

@@ -33,7 +33,8 @@ __all__ = [
     "DeviceMatblock",
     "MatrixFreeRealSymOp", "chebyshev_poly_real_symm_sparse", "polfed", "gershgorin_bounds",
     "jackson_kernel", "cheb_delta_coeffs", "cheb_window_coeffs", "cheb_smooth_window_coeffs",
-    "build_coeffs", "apply_poly_block", "lanczos_bounds", "ArgumentError", "SMAError",
+    "build_coeffs", "apply_poly_block", "lanczos_bounds", "polfed_windows", "ArgumentError",
+    "SMAError",
 ]
 
 ArgumentError = L.ArgumentError
@@ -348,15 +349,18 @@ def _op_of(A) -> _DeviceOp:
 
 
 # ====================================================================== results
-def _take_result(hres: ctypes.c_void_p, stats: Optional[dict]):
+def _take_result(hres: ctypes.c_void_p, stats: Optional[dict], vectors: bool = True):
+    """(lam, X, res) of a result handle, which is freed.  ``vectors=False`` leaves the
+    eigenvectors on the device (X is None): no n x k download."""
     lib = L.load()
     try:
         k, n = ctypes.c_int64(), ctypes.c_int64()
         L.check(lib.sma_result_count(hres, ctypes.byref(k), ctypes.byref(n)))
         lam = np.empty(k.value)
         res = np.empty(k.value)
-        X = np.empty((n.value, k.value), order="F")
-        L.check(lib.sma_result_copy(hres, lam.ctypes.data, X.ctypes.data if X.size else None,
+        X = np.empty((n.value, k.value), order="F") if vectors else None
+        L.check(lib.sma_result_copy(hres, lam.ctypes.data,
+                                    X.ctypes.data if X is not None and X.size else None,
                                     res.ctypes.data))
         if stats is not None:
             st = L.Stats()
@@ -430,7 +434,7 @@ def polfed(A, *args, s: int = 8, smin=None, smax=None, sigma: float = 0.0,
            window_type="step", jackson: bool = True, mmax: Optional[int] = None,
            rtol: float = 1e-12, reorth_passes: int = 1, extra_keep: int = 8, seed: int = 1,
            show_progress: bool = False, chunk: int = 64, precision: str = "fp64",
-           stats: Optional[dict] = None, **kw):
+           stats: Optional[dict] = None, vectors: bool = True, **kw):
     """POLFED: block Lanczos on the Chebyshev-filtered operator (``polfed.jl:1128``).
 
     ``polfed(A, nev, degree; ...)`` with a :class:`MatrixFreeRealSymOp` (or, as an
@@ -438,7 +442,8 @@ def polfed(A, *args, s: int = 8, smin=None, smax=None, sigma: float = 0.0,
     ``polfed(matvec, n, nev, degree; matblock=...)`` (``polfed.jl:1183``; ``matblock!``
     may be spelled ``matblock``).  ``smin``/``smax`` are required.  The return order
     follows ``polfed.jl:1148-1157``: by eigenvalue when the nev-th smallest residual is
-    below ``tol``, else the nev best by residual.
+    below ``tol``, else the nev best by residual.  ``vectors=False`` returns X as None
+    (the eigenvectors are not copied to the host).
     """
     matblock = kw.pop("matblock!", kw.pop("matblock", None))
     if kw:
@@ -465,7 +470,60 @@ def polfed(A, *args, s: int = 8, smin=None, smax=None, sigma: float = 0.0,
     h = ctypes.c_void_p()
     L.check(L.load().sma_polfed_solve(op.handle, int(nev), int(degree), ctypes.byref(o),
                                       ctypes.byref(h)))
-    return _take_result(h, stats)
+    return _take_result(h, stats, vectors)
+
+
+# ====================================================================== batched POLFED
+def polfed_windows(A, windows, nevs, degrees, mmaxs, *, s: int = 8, smin=None, smax=None,
+                   tol: float = 1e-10, overextract: int = 2, refine: bool = True,
+                   window_type="step", jackson: bool = True, rtol: float = 1e-12,
+                   reorth_passes: int = 1, extra_keep: int = 8, seed: int = 1,
+                   show_progress: bool = False, precision: str = "fp64",
+                   stats: Optional[dict] = None, vectors: bool = True):
+    """Batched POLFED (an extension; the reference runs ``polfed`` on one window per call):
+    window ``w`` = ``windows[w]`` is a POLFED solve with ``nevs[w]``, ``degrees[w]`` and
+    ``mmaxs[w]`` (its filter centred on the window, seed ``seed + w``), and every block step
+    filters all windows' blocks in ONE segmented recurrence.  Returns
+    ``(lam, X, res, win)``: per window its pairs in polfed's return order, windows in
+    order, ``win[j]`` the window of pair ``j``.  ``stats`` also receives
+    ``window_blocks`` and ``window_by_lambda`` (the return rule's branch) per window."""
+    op = A if isinstance(A, _DeviceOp) else _resolve_sparse(A)
+    w = np.asarray(windows, dtype=np.float64).reshape(-1, 2)
+    emin = np.ascontiguousarray(w[:, 0])
+    emax = np.ascontiguousarray(w[:, 1])
+    nev = np.ascontiguousarray(nevs, dtype=np.int64)
+    deg = np.ascontiguousarray(degrees, dtype=np.int64)
+    mm = np.ascontiguousarray(mmaxs, dtype=np.int64)
+    if not (nev.size == deg.size == mm.size == emin.size):
+        raise ArgumentError(L.SMA_ERR_ARG, "windows, nevs, degrees and mmaxs differ in length")
+    if smin is None or smax is None:
+        raise ArgumentError(L.SMA_ERR_BOUNDS, "Matrix-free POLFED requires spectral bounds smin and smax")
+    o = L.PolfedOpts()
+    lib = L.load()
+    lib.sma_polfed_opts_default(ctypes.byref(o))
+    o.s, o.smin, o.smax, o.has_bounds = int(s), float(smin), float(smax), 1
+    o.tol, o.overextract, o.refine = float(tol), int(overextract), int(refine)
+    o.window_type, o.jackson = _window(window_type), int(jackson)
+    o.rtol, o.reorth_passes, o.extra_keep = float(rtol), int(reorth_passes), int(extra_keep)
+    o.seed, o.show_progress = int(seed), int(show_progress)
+    o.precision = L.PRECISIONS[precision]
+    h = ctypes.c_void_p()
+    L.check(lib.sma_polfed_batch_solve(op.handle, int(emin.size), emin.ctypes.data,
+                                       emax.ctypes.data, nev.ctypes.data, deg.ctypes.data,
+                                       mm.ctypes.data, ctypes.byref(o), ctypes.byref(h)))
+    k = ctypes.c_int64()
+    L.check(lib.sma_result_count(h, ctypes.byref(k), None))
+    win = np.zeros(k.value, dtype=np.int64)
+    if k.value:
+        L.check(lib.sma_result_windows(h, win.ctypes.data))
+    if stats is not None:
+        its = np.zeros(emin.size, dtype=np.int64)
+        conv = np.zeros(emin.size, dtype=np.int64)
+        L.check(lib.sma_result_window_info(h, int(emin.size), its.ctypes.data, conv.ctypes.data))
+        stats["window_blocks"] = its
+        stats["window_by_lambda"] = conv.astype(bool)
+    lam, X, res = _take_result(h, stats, vectors)
+    return lam, X, res, win
 
 
 # ====================================================================== batched slicing

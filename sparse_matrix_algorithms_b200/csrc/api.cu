@@ -11,6 +11,9 @@
 namespace sma {
 sma_result *cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts &o);
 sma_result *polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polfed_opts &o);
+sma_result *polfed_batch_solve(sma_op *op, int64_t nwin, const double *emin, const double *emax,
+                               const int64_t *nev, const int64_t *degree, const int64_t *mmax,
+                               const sma_polfed_opts &o);
 sma_result *slice_solve(sma_op *op, int64_t nwin, const double *emin, const double *emax,
                         const int64_t *degree, const int64_t *m0, const sma_slice_opts &o);
 
@@ -102,6 +105,8 @@ int sma_ctx_create(int device, sma_ctx **out) {
     ctx->filter_graphs = !(fg && std::string(fg) == "0");
     const char *pe = std::getenv("SMA_PERSISTENT");
     ctx->persistent = pe && std::string(pe) == "1";
+    const char *cd = std::getenv("SMA_CUBLAS_DENSE");
+    ctx->cublas_dense = cd && std::string(cd) == "1";
     try {
       SMA_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
       SMA_CUBLAS(cublasCreate(&ctx->cublas));
@@ -228,16 +233,15 @@ int sma_op_create_csc_upper(sma_ctx *ctx, int64_t n, int64_t nnz, const int64_t 
     *out = nullptr;
     std::vector<int> rp, ci;
     validate_csc(n, nnz, colptr, rowval, nzval, index_base, rp, ci);
-    // column j of a symmetric CSC is row j: Gershgorin over the full rows, optional exact
-    // symmetry check (a_ij == a_ji for every stored entry), then the upper triangle
-    double gmin = INFINITY, gmax = -INFINITY;
+    // column j of a symmetric CSC is row j: optional exact symmetry check (a_ij == a_ji
+    // for every stored entry), then the upper triangle.  The operator applied is
+    // U + U^T - D whatever the lower triangle held, so its Gershgorin bounds come from the
+    // kept entries: each off-diagonal u_ji counts in row j and in row i.
     std::vector<int> urp(n + 1, 0), uci;
-    std::vector<double> uval;
+    std::vector<double> uval, diag(n, 0.0), off(n, 0.0);
     for (int64_t j = 0; j < n; ++j) {
-      double diag = 0.0, off = 0.0;
       for (int t = rp[j]; t < rp[j + 1]; ++t) {
         const int i = ci[t];
-        if (i == j) diag = nzval[t]; else off += std::fabs(nzval[t]);
         if (check_symmetric && i != j) {
           const int *b = ci.data() + rp[i], *e = ci.data() + rp[i + 1];
           const int *p = std::lower_bound(b, e, (int)j);
@@ -247,11 +251,20 @@ int sma_op_create_csc_upper(sma_ctx *ctx, int64_t n, int64_t nnz, const int64_t 
         if (i >= j) {
           uci.push_back(i);
           uval.push_back(nzval[t]);
+          if (i == j) {
+            diag[j] = nzval[t];
+          } else {
+            off[j] += std::fabs(nzval[t]);
+            off[i] += std::fabs(nzval[t]);
+          }
         }
       }
-      gmin = std::min(gmin, diag - off);
-      gmax = std::max(gmax, diag + off);
       urp[j + 1] = (int)uci.size();
+    }
+    double gmin = INFINITY, gmax = -INFINITY;
+    for (int64_t j = 0; j < n; ++j) {
+      gmin = std::min(gmin, diag[j] - off[j]);
+      gmax = std::max(gmax, diag[j] + off[j]);
     }
     const int64_t unnz = (int64_t)uci.size();
     DeviceGuard g(ctx->device);
@@ -420,6 +433,92 @@ int sma_apply_poly_block_dev(sma_op *op, const double *coeffs, int64_t K, double
   });
 }
 
+int sma_apply_poly_block_percol_dev(sma_op *op, const double *coeffs, int64_t K, double smin,
+                                    double smax, const void *Q_dev, void *Y_dev, int64_t b,
+                                    int64_t precision) {
+  return guarded([&] {
+    check_op(op);
+    require(coeffs != nullptr && K >= 0, SMA_ERR_ARG, "coefficients: need K >= 0 and (K+1) x b values");
+    check_bounds(smin, smax);
+    require(b >= 0, SMA_ERR_ARG, "negative block width");
+    require(precision == SMA_PREC_FP64 || precision == SMA_PREC_FP32, SMA_ERR_ARG, "unknown precision");
+    require(op->kind != OP_MATBLOCK, SMA_ERR_ARG, "the per-column filter needs a device operator");
+    const int64_t n = op->n;
+    if (n == 0 || b == 0) return;
+    require(Q_dev && Y_dev, SMA_ERR_ARG, "null block pointer");
+    for (int64_t i = 0; i < (K + 1) * b; ++i)
+      require(std::isfinite(coeffs[i]), SMA_ERR_ARG, "non-finite coefficient");
+    DeviceGuard g(op->ctx->device);
+    cudaStream_t st = op->ctx->stream;
+    std::vector<int> idn(b);
+    for (int64_t j = 0; j < b; ++j) idn[j] = (int)j;
+    DevBuf<int> colseg(b, st);
+    SMA_CUDA(cudaMemcpyAsync(colseg.p, idn.data(), b * sizeof(int), cudaMemcpyHostToDevice, st));
+    auto run = [&](auto zero) {
+      using T = decltype(zero);
+      std::vector<T> ch((K + 1) * b);
+      for (int64_t i = 0; i < (K + 1) * b; ++i) ch[i] = (T)coeffs[i];
+      DevBuf<T> coef(ch.size(), st), B1(n * b, st), B2(n * b, st), TMP(n * b, st), AX;
+      if (op->kind != OP_CSR) AX.alloc(n * b, st);
+      SMA_CUDA(cudaMemcpyAsync(coef.p, ch.data(), ch.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+      percol_filter<T>(op, st, coef.p, K, smin, smax, (const T *)Q_dev, (T *)Y_dev, b, colseg.p,
+                       B1.p, B2.p, TMP.p, AX.p);
+      SMA_CUDA(cudaStreamSynchronize(st));
+    };
+    if (precision == SMA_PREC_FP64) {
+      run(0.0);
+    } else {
+      if ((op->kind == OP_CSR || op->kind == OP_CSR_HALF) && !op->val32) {
+        SMA_CUDA(cudaMalloc((void **)&op->val32, std::max<int64_t>(op->nnz, 1) * sizeof(float)));
+        launch_copy_block<double, float>(st, op->nnz, 1, op->val64, 1, op->val32, 1);
+      }
+      run(0.0f);
+    }
+  });
+}
+
+int sma_dense_gram_dev(sma_ctx *ctx, int64_t n, int64_t m, int64_t k, const double *X_dev,
+                       int64_t ldx, const double *Y_dev, int64_t ldy, double *C_dev, int64_t ldc,
+                       double alpha, double beta) {
+  return guarded([&] {
+    check_ctx(ctx);
+    require(n >= 0 && m >= 0 && k >= 0 && ldx >= m && ldy >= k && ldc >= std::max<int64_t>(m, 1),
+            SMA_ERR_ARG, "bad sizes or leading dimensions");
+    if (m == 0 || k == 0) return;
+    require(C_dev && (n == 0 || (X_dev && Y_dev)), SMA_ERR_ARG, "null block pointer");
+    DeviceGuard g(ctx->device);
+    Dense dn(ctx);
+    dn.gram(n, m, k, X_dev, ldx, Y_dev, ldy, C_dev, ldc, alpha, beta);
+    SMA_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int sma_dense_update_dev(sma_ctx *ctx, int64_t n, int64_t m, int64_t p, const double *X_dev,
+                         int64_t ldx, const double *C_dev, int64_t ldc, int64_t transC,
+                         double *Y_dev, int64_t ldy, double alpha, double beta) {
+  return guarded([&] {
+    check_ctx(ctx);
+    require(n >= 0 && m >= 0 && p >= 0 && ldx >= m && ldy >= p &&
+                ldc >= std::max<int64_t>(transC ? p : m, 1),
+            SMA_ERR_ARG, "bad sizes or leading dimensions");
+    if (n == 0 || p == 0) return;
+    require(Y_dev && (m == 0 || (X_dev && C_dev)), SMA_ERR_ARG, "null block pointer");
+    DeviceGuard g(ctx->device);
+    Dense dn(ctx);
+    dn.mul_small(n, m, p, X_dev, ldx, C_dev, ldc, Y_dev, ldy, alpha, beta, transC != 0);
+    SMA_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int sma_divided_difference(const double *coeffs, int64_t K, double t, double *e, double *pt) {
+  return guarded([&] {
+    require(coeffs != nullptr && e != nullptr && pt != nullptr && K >= 1, SMA_ERR_ARG,
+            "need K >= 1, K+1 coefficients and K outputs");
+    std::vector<double> c(coeffs, coeffs + K + 1);
+    divided_difference(c, t, e, pt);
+  });
+}
+
 int sma_apply_poly_block(sma_op *op, const double *coeffs, int64_t K, double smin, double smax,
                          const double *Q, double *Y, int64_t b, int64_t precision) {
   return guarded([&] {
@@ -557,6 +656,24 @@ int sma_polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polfed_o
     if (o.has_bounds) check_bounds(o.smin, o.smax);
     DeviceGuard g(op->ctx->device);
     *out = polfed_solve(op, nev, degree, o);
+  });
+}
+
+int sma_polfed_batch_solve(sma_op *op, int64_t nwin, const double *emin, const double *emax,
+                           const int64_t *nev, const int64_t *degree, const int64_t *mmax,
+                           const sma_polfed_opts *opts, sma_result **out) {
+  return guarded([&] {
+    check_op(op);
+    require(out != nullptr, SMA_ERR_ARG, "null output pointer");
+    *out = nullptr;
+    sma_polfed_opts o;
+    if (opts) o = *opts; else sma_polfed_opts_default(&o);
+    require(o.precision == SMA_PREC_FP64 || o.precision == SMA_PREC_FP32 ||
+                o.precision == SMA_PREC_MIXED, SMA_ERR_ARG, "unknown precision");
+    if (o.has_bounds) check_bounds(o.smin, o.smax);
+    require(nwin >= 1 && nwin <= 4096, SMA_ERR_ARG, "nwin must be in 1..4096");
+    DeviceGuard g(op->ctx->device);
+    *out = polfed_batch_solve(op, nwin, emin, emax, nev, degree, mmax, o);
   });
 }
 

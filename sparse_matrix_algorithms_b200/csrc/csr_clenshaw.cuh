@@ -34,17 +34,30 @@ constexpr int kStage = 1024;  // CSR entries a STAGED CTA keeps in shared memory
 
 template <typename T, int V, bool HQ, bool HS, bool HB>
 __device__ __forceinline__ void epilogue(T *__restrict__ out, const T (&acc)[V], const T (&q)[V],
-                                         const T (&s)[V], const T (&t)[V], T ck, T alpha, T beta) {
+                                         const T (&s)[V], const T (&t)[V], const T (&ck)[V],
+                                         T alpha, T beta) {
   T r[V];
 #pragma unroll
   for (int v = 0; v < V; ++v) {
     T x = alpha * acc[v];
-    if constexpr (HQ) x = ck * q[v] + x;
+    if constexpr (HQ) x = ck[v] * q[v] + x;
     if constexpr (HS) x = x + beta * s[v];
     if constexpr (HB) x = x - t[v];
     r[v] = x;
   }
   stv<T, V>(out, r);
+}
+
+// The Q coefficient of each of a thread's V columns c0 .. c0+V-1: the step's scalar ck, or
+// (PC) the coefficient of the column's segment, cseg[colseg[c]].
+template <typename T, int V, bool PC>
+__device__ __forceinline__ void coeffs_of(T (&ckv)[V], T ck, const T *__restrict__ cseg,
+                                          const int *__restrict__ colseg, int c0) {
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    if constexpr (PC) ckv[v] = __ldg(cseg + __ldg(colseg + c0 + v));
+    else ckv[v] = ck;
+  }
 }
 
 // R consecutive entries from j: all R gathers are issued before the first FMA, so R
@@ -95,7 +108,7 @@ direct_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
               const T *__restrict__ val, int64_t n, int b, const T *__restrict__ Q, int64_t ldq,
               const T *__restrict__ B1, const T *__restrict__ B2, int64_t ldb,
               T *__restrict__ out, int64_t ldo, T ck, T alpha, T beta,
-              const T *__restrict__ cseg, const int *__restrict__ colseg8) {
+              const T *__restrict__ cseg, const int *__restrict__ colseg) {
   constexpr int kRows = kThreads / G;
   const int64_t row = (int64_t)blockIdx.x * kRows + threadIdx.x / G;
   if (row >= n) return;
@@ -110,9 +123,9 @@ direct_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
     if constexpr (HS) ldv<T, V>(B1 + row * ldb + c0, s);
     if constexpr (HB) ldv<T, V>(B2 + row * ldb + c0, t);
     row_product<T, V, U>(colind, val, 0, start, end, B1 + c0, ldb, acc);
-    T ckc = ck;
-    if constexpr (PC) ckc = __ldg(cseg + __ldg(colseg8 + (c0 >> 3)));
-    epilogue<T, V, HQ, HS, HB>(out + row * ldo + c0, acc, q, s, t, ckc, alpha, beta);
+    T ckv[V];
+    coeffs_of<T, V, PC>(ckv, ck, cseg, colseg, c0);
+    epilogue<T, V, HQ, HS, HB>(out + row * ldo + c0, acc, q, s, t, ckv, alpha, beta);
   }
 }
 
@@ -122,7 +135,7 @@ staged_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
               const T *__restrict__ val, int64_t n, int b, const T *__restrict__ Q, int64_t ldq,
               const T *__restrict__ B1, const T *__restrict__ B2, int64_t ldb,
               T *__restrict__ out, int64_t ldo, T ck, T alpha, T beta,
-              const T *__restrict__ cseg, const int *__restrict__ colseg8) {
+              const T *__restrict__ cseg, const int *__restrict__ colseg) {
   constexpr int kRows = kThreads / G;
   __shared__ int s_col[kStage];
   __shared__ T s_val[kStage];
@@ -152,9 +165,9 @@ staged_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
     if constexpr (HB) ldv<T, V>(B2 + row * ldb + c0, t);
     if (staged) row_product<T, V, U>(s_col, s_val, base, start, end, B1 + c0, ldb, acc);
     else row_product<T, V, U>(colind, val, 0, start, end, B1 + c0, ldb, acc);
-    T ckc = ck;
-    if constexpr (PC) ckc = __ldg(cseg + __ldg(colseg8 + (c0 >> 3)));
-    epilogue<T, V, HQ, HS, HB>(out + row * ldo + c0, acc, q, s, t, ckc, alpha, beta);
+    T ckv[V];
+    coeffs_of<T, V, PC>(ckv, ck, cseg, colseg, c0);
+    epilogue<T, V, HQ, HS, HB>(out + row * ldo + c0, acc, q, s, t, ckv, alpha, beta);
   }
 }
 
@@ -218,7 +231,9 @@ async_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
       if constexpr (HS) s[v] = reinterpret_cast<const T *>(&buf[NB + 1][tid])[v];
       if constexpr (HB) t[v] = reinterpret_cast<const T *>(&buf[NB + 2][tid])[v];
     }
-    epilogue<T, V, HQ, HS, HB>(out + row * ldo + c0, acc, q, s, t, ck, alpha, beta);
+    T ckv[V];
+    coeffs_of<T, V, false>(ckv, ck, nullptr, nullptr, c0);
+    epilogue<T, V, HQ, HS, HB>(out + row * ldo + c0, acc, q, s, t, ckv, alpha, beta);
   }
 }
 
@@ -242,10 +257,11 @@ struct Args {
   T *out;
   int64_t ldo;
   double ck, alpha, beta;
-  // batched spectrum slicing: per-segment coefficients of this step (cseg[segment]) and the
-  // segment of every 8 consecutive columns (colseg8[column / 8]); null for one segment
+  // per-segment coefficients of this step (cseg[segment]) and the segment of every column
+  // (colseg[column]); null for one coefficient.  Batched spectrum slicing maps a window's
+  // columns to its segment; the POLFED polish gives every column its own polynomial.
   const T *cseg = nullptr;
-  const int *colseg8 = nullptr;
+  const int *colseg = nullptr;
 };
 
 template <typename T, int V, int G, int U, bool HQ, bool HS, bool HB>
@@ -260,11 +276,11 @@ void launch_one(int fam, const Args<T> &a) {
       if (fam == 0)
         direct_kernel<T, V, G, U, true, true, true, true><<<grid, kThreads, 0, a.st>>>(
             a.op->rowptr, a.op->colind, val, a.op->n, (int)a.b, a.Q, a.ldq, a.B1, a.B2, a.ldb,
-            a.out, a.ldo, T(0), (T)a.alpha, (T)a.beta, a.cseg, a.colseg8);
+            a.out, a.ldo, T(0), (T)a.alpha, (T)a.beta, a.cseg, a.colseg);
       else
         staged_kernel<T, V, G, U, true, true, true, true><<<grid, kThreads, 0, a.st>>>(
             a.op->rowptr, a.op->colind, val, a.op->n, (int)a.b, a.Q, a.ldq, a.B1, a.B2, a.ldb,
-            a.out, a.ldo, T(0), (T)a.alpha, (T)a.beta, a.cseg, a.colseg8);
+            a.out, a.ldo, T(0), (T)a.alpha, (T)a.beta, a.cseg, a.colseg);
       SMA_CHECK_LAUNCH();
       return;
     }
@@ -493,18 +509,17 @@ void csr_clenshaw_step_untuned(const sma_op *op, cudaStream_t st, int64_t b, con
   throw Error(SMA_ERR_INTERNAL, "unsupported Clenshaw step variant");
 }
 
-// The segmented step of batched spectrum slicing: column c takes the coefficient
-// cseg[colseg8[c / 8]]; Q, B1 and B2 are all read.  tuned = false uses the operator's
-// cached configuration (or the default one) and creates no events, so that it may be
-// recorded into a CUDA graph.
+// The segmented step: column c takes the coefficient cseg[colseg[c]]; Q, B1 and B2 are all
+// read.  tuned = false uses the operator's cached configuration (or the default one) and
+// creates no events, so that it may be recorded into a CUDA graph.
 template <typename T>
 void csr_clenshaw_step_seg(const sma_op *op, cudaStream_t st, int64_t b, const T *Q, int64_t ldq,
                            const T *B1, const T *B2, int64_t ldb, T *out, int64_t ldo,
-                           const T *cseg, const int *colseg8, double alpha, double beta,
+                           const T *cseg, const int *colseg, double alpha, double beta,
                            bool tuned) {
   csr::Args<T> a{op, st, b, Q, ldq, B1, B2, ldb, out, ldo, 0.0, alpha, beta};
   a.cseg = cseg;
-  a.colseg8 = colseg8;
+  a.colseg = colseg;
   if (tuned) return csr::step<T, true, true, true>(a);
   csr::step_untuned<T, true, true, true>(a);
 }

@@ -28,6 +28,10 @@ namespace sma {
 void Dense::gram(int64_t n, int64_t m, int64_t k, const double *X, int64_t ldx, const double *Y,
                  int64_t ldy, double *C, int64_t ldc, double alpha, double beta) {
   if (m == 0 || k == 0) return;
+  if (!ctx->cublas_dense) {
+    dgemm_gram(ctx->stream, ctx->num_sms, n, m, k, X, ldx, Y, ldy, C, ldc, alpha, beta, work);
+    return;
+  }
   SMA_CUBLAS(cublasDgemm(ctx->cublas, CUBLAS_OP_N, CUBLAS_OP_T, (int)m, (int)k, (int)n, &alpha, X,
                          (int)ldx, Y, (int)ldy, &beta, C, (int)ldc));
 }
@@ -36,6 +40,10 @@ void Dense::mul_small(int64_t n, int64_t m, int64_t p, const double *X, int64_t 
                       const double *C, int64_t ldc, double *Y, int64_t ldy, double alpha,
                       double beta, bool transC) {
   if (p == 0 || n == 0) return;
+  if (!ctx->cublas_dense) {
+    dgemm_update(ctx->stream, ctx->num_sms, n, m, p, X, ldx, C, ldc, transC, Y, ldy, alpha, beta);
+    return;
+  }
   if (m == 0) {  // Y = beta*Y
     const double zero = 0.0;
     if (beta != 1.0)
@@ -80,13 +88,30 @@ int potrf_upper(sma_ctx *ctx, int64_t k, double *G, int64_t ldg) {
   return h;
 }
 
-// X <- X R^{-1} for row-major X (n x k) and upper-triangular R (k x k column-major):
-// on X^T (column-major k x n) this is X^T <- R^{-T} X^T.
+// X <- X R^{-1} for row-major X (n x k) and upper-triangular R (k x k column-major).
+// This library's path: R^{-1} (k x k, a triangular solve against the identity -- tiny) and
+// then one tensor-core product X R^{-1}, in place when k <= 64, else through a copy.  With
+// SMA_CUBLAS_DENSE=1: cuBLAS DTRSM on X^T (column-major k x n), X^T <- R^{-T} X^T.
 void trsm_right_upper(sma_ctx *ctx, int64_t n, int64_t k, const double *R, int64_t ldr, double *X,
                       int64_t ldx) {
   const double one = 1.0;
-  SMA_CUBLAS(cublasDtrsm(ctx->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T,
-                         CUBLAS_DIAG_NON_UNIT, (int)k, (int)n, &one, R, (int)ldr, X, (int)ldx));
+  if (ctx->cublas_dense) {
+    SMA_CUBLAS(cublasDtrsm(ctx->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T,
+                           CUBLAS_DIAG_NON_UNIT, (int)k, (int)n, &one, R, (int)ldr, X, (int)ldx));
+    return;
+  }
+  cudaStream_t st = ctx->stream;
+  DevBuf<double> Rinv(k * k, st);
+  launch_identity(st, k, Rinv.p, k);
+  SMA_CUBLAS(cublasDtrsm(ctx->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                         CUBLAS_DIAG_NON_UNIT, (int)k, (int)k, &one, R, (int)ldr, Rinv.p, (int)k));
+  if (k <= 64) {
+    dgemm_update(st, ctx->num_sms, n, k, k, X, ldx, Rinv.p, k, false, X, ldx, 1.0, 0.0);
+  } else {
+    DevBuf<double> tmp(n * k, st);
+    dgemm_update(st, ctx->num_sms, n, k, k, X, ldx, Rinv.p, k, false, tmp.p, k, 1.0, 0.0);
+    launch_copy_block<double, double>(st, n, k, tmp.p, k, X, ldx);
+  }
 }
 
 std::vector<double> to_host(sma_ctx *ctx, const double *d, size_t count) {

@@ -463,6 +463,15 @@ __global__ void zero_lower_kernel(int64_t k, double *G, int64_t ld) {
   }
 }
 
+__global__ void identity_kernel(int64_t k, double *G, int64_t ld) {
+  const int64_t total = k * k;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t % k, j = t / k;
+    G[i + j * ld] = i == j ? 1.0 : 0.0;
+  }
+}
+
 // ------------------------------------------------------------------ CSR checks
 __global__ void gershgorin_kernel(int64_t n, const int *__restrict__ rowptr,
                                   const int *__restrict__ colind, const double *__restrict__ val,
@@ -682,6 +691,12 @@ void launch_add_diagonal(cudaStream_t st, int64_t k, double *G, int64_t ld, doub
 void launch_zero_lower(cudaStream_t st, int64_t k, double *G, int64_t ld) {
   if (k == 0) return;
   zero_lower_kernel<<<grid_for(k * k), 256, 0, st>>>(k, G, ld);
+  SMA_CHECK_LAUNCH();
+}
+
+void launch_identity(cudaStream_t st, int64_t k, double *G, int64_t ld) {
+  if (k == 0) return;
+  identity_kernel<<<grid_for(k * k), 256, 0, st>>>(k, G, ld);
   SMA_CHECK_LAUNCH();
 }
 

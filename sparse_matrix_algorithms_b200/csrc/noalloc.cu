@@ -19,7 +19,8 @@
 //    array; callers serialize them;
 //  * the first call on a device looks the array's device address up (cudaGetSymbolAddress
 //    with that device current) and caches it; make that first call before any stream
-//    capture.
+//    capture.  cudaDeviceReset ends every context of this library on that device, this
+//    cached address included.
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -88,8 +89,11 @@ void filter_noalloc(sma_op *op, const double *coeffs, int64_t K, double smin, do
   require(std::isfinite(smin) && std::isfinite(smax) && smin < smax, SMA_ERR_ARG,
           "spectral bounds must satisfy smin < smax");
   require(b >= 0 && ldq >= b && ldy >= b, SMA_ERR_ARG, "leading dimensions must be >= b");
-  require(op->kind == OP_CSR || op->kind == OP_LAP1D, SMA_ERR_ARG,
-          "the allocation-free filter takes device operators (CSR, stencil) only");
+  require(op->kind == OP_CSR || op->kind == OP_LAP1D || op->kind == OP_ANDERSON ||
+              op->kind == OP_XXZ,
+          SMA_ERR_ARG,
+          "the allocation-free filter takes a CSR matrix or a model stencil (1D Laplacian, "
+          "Anderson, XXZ); half storage and caller callbacks are not accepted");
   const int64_t n = op->n;
   if (n == 0 || b == 0) return;
   require(Q != nullptr && Y != nullptr, SMA_ERR_ARG, "null block pointer");

@@ -12,10 +12,12 @@
 // launch, and L1 is not coherent across SMs, so every read of them goes through L2
 // (ld.global.cg); Q and the CSR arrays are read-only during the launch (ld.global.nc).
 //
-// The grid barrier is a counter plus a generation word.  Its wait is bounded: a CTA that
-// spins longer than the limit (about a second), or sees another CTA's error flag, sets
-// the error flag and returns; the host reads the flag after the launch and reports
-// SMA_ERR_TIMEOUT.  The launch is cooperative (cudaLaunchCooperativeKernel), so all CTAs
+// The grid barrier is a counter plus a generation word.  Its wait is bounded by elapsed
+// time, read from the %globaltimer nanosecond clock: a CTA that has waited longer than the
+// limit (one second for the filter), or sees another CTA's error flag, sets the error flag
+// and returns; the host reads the flag after the launch and reports SMA_ERR_TIMEOUT.  A
+// spin count far beyond any real wait backs the clock up, so the loop ends even if the
+// clock stood still.  The launch is cooperative (cudaLaunchCooperativeKernel), so all CTAs
 // are co-resident or the launch fails without running.
 #include <cuda_runtime.h>
 
@@ -91,8 +93,18 @@ struct Barrier {
   unsigned *gen;
   int *err;
   unsigned nblocks;
-  unsigned long long max_spin;
+  unsigned long long max_wait_ns;  // give up after this much elapsed time
 };
+
+// Spins of 100 ns sleeps after which a wait gives up whatever the clock says (2^34 spins
+// take far longer than any wait limit used here).
+constexpr unsigned long long kSpinBackstop = 1ull << 34;
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 // All CTAs meet; returns false (in every thread of the CTA) when the wait gave up.
 __device__ __forceinline__ bool grid_sync(const Barrier &bar) {
@@ -109,8 +121,10 @@ __device__ __forceinline__ bool grid_sync(const Barrier &bar) {
       atomicAdd(bar.gen, 1u);
     } else {
       unsigned long long spins = 0;
+      const unsigned long long t0 = globaltimer_ns();
       while (*reinterpret_cast<volatile unsigned *>(bar.gen) == g) {
-        if (++spins > bar.max_spin || *reinterpret_cast<volatile int *>(bar.err) != 0) {
+        if (globaltimer_ns() - t0 > bar.max_wait_ns || ++spins > kSpinBackstop ||
+            *reinterpret_cast<volatile int *>(bar.err) != 0) {
           atomicExch(bar.err, 1);
           ok = 0;
           break;
@@ -209,7 +223,7 @@ int launch(const sma_op *op, cudaStream_t st, int64_t b, const T *Q, int64_t ldq
   else val = (const T *)op->val32;
   int n = (int)op->n, bi = (int)b, Ki = K;
   T a = (T)alpha, bt = (T)beta, id = (T)invd, bl = (T)beta_last;
-  Barrier bar{barrier_words, barrier_words + 1, err, grid, 10000000ull};  // ~1 s of 100 ns sleeps
+  Barrier bar{barrier_words, barrier_words + 1, err, grid, 1000000000ull};  // 1 s
   void *args[] = {(void *)&op->rowptr, (void *)&op->colind, (void *)&val, &n, &bi, (void *)&Q,
                   &ldq, &buf0, &buf1, &buf2, &Y, &ldy, (void *)&coeffs, &Ki, &a, &bt, &id, &bl,
                   &bar};
@@ -287,7 +301,7 @@ __global__ void barrier_selftest_kernel(Barrier bar) {
 }
 }  // namespace persist
 
-// Runs the barrier with one CTA missing and a ~10 ms spin limit; returns SMA_ERR_TIMEOUT
+// Runs the barrier with one CTA missing and a 10 ms wait limit; returns SMA_ERR_TIMEOUT
 // when the wait gave up and reported it through the error flag (the expected outcome).
 int barrier_selftest(sma_ctx *ctx) {
   cudaStream_t st = ctx->stream;
@@ -295,7 +309,7 @@ int barrier_selftest(sma_ctx *ctx) {
   SMA_CUDA(cudaMemsetAsync(words.p, 0, 3 * sizeof(unsigned), st));
   const unsigned launched = 2;
   persist::Barrier bar{words.p, words.p + 1, reinterpret_cast<int *>(words.p + 2), launched + 1,
-                       100000ull};
+                       10000000ull};  // 10 ms
   void *args[] = {&bar};
   SMA_CUDA(cudaLaunchCooperativeKernel((const void *)persist::barrier_selftest_kernel,
                                        dim3(launched), dim3(persist::kThreads), args, 0, st));

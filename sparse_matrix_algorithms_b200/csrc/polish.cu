@@ -1,0 +1,230 @@
+// FP64 polish of Ritz vectors at FP32 cost (POLFED in MIXED precision).
+//
+// An FP32-filtered POLFED basis yields Ritz vectors whose residuals stop near 1e-6 of the
+// spectral scale: the FP32 rounding of every filtered block enters the Krylov basis.  The
+// polish refines them by subspace iteration with the same filter polynomial p, but
+// never applies p in FP32 to the vectors themselves.  For a unit vector x with Rayleigh
+// quotient theta and residual r = (A - theta) x, the divided difference
+//
+//     q_t(s) = (p(s) - p(t)) / (s - t),   t = (theta - c) / d   (A_hat = (A - c) / d)
+//
+// is a polynomial of degree K - 1 and
+//
+//     p(A_hat) x = p(t) x + q_t(A_hat) r / d.
+//
+// The first term is exact in FP64; the second applies q_t in FP32 to r / ||r||, so its
+// rounding error is ~1e-7 of ||r|| / d instead of ~1e-7 of ||x||: the filtered block comes
+// out with FP64-level accuracy while the recurrence streams FP32 blocks.  Each column has
+// its own t, so every column runs its own polynomial: one segmented Clenshaw recurrence
+// with one coefficient segment per column.  The coefficients of q_t are the Clenshaw
+// intermediates of p at t: with b_m = c_m + 2 t b_{m+1} - b_{m+2} (b_{K+1} = b_{K+2} = 0),
+// q_t = b_1 T_0 + sum_{m>=2} 2 b_m T_{m-1} and p(t) = c_0 + t b_1 - b_2 (synthetic division
+// by (s - t) in the Chebyshev basis).
+//
+// One pass: residuals, the FP32 per-column recurrence, Y = p(t) X + Z diag(||r|| / d) in
+// FP64, orthonormalization (CholQR2) and Rayleigh-Ritz with A, all in FP64.  The reference's
+// only post-processing is Rayleigh-Ritz (refine_original_rr, polfed.jl:837-880); this
+// filtered pass is what an FP32 basis needs on top of it to reach its tolerance.
+#include <cmath>
+
+#include "solver_common.h"
+
+namespace sma {
+namespace {
+
+// R32[i, j] = (AX[i, j] - theta[j] X[i, j]) * inv_s[j] for j < k, 0 for k <= j < kpad.
+__global__ void residual_f32_kernel(int64_t n, int64_t k, int64_t kpad, const double *__restrict__ X,
+                                    int64_t ldx, const double *__restrict__ AX, int64_t ldax,
+                                    const double *__restrict__ theta,
+                                    const double *__restrict__ inv_s, float *__restrict__ R,
+                                    int64_t ldr) {
+  const int64_t total = n * kpad;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t / kpad, j = t % kpad;
+    float v = 0.f;
+    if (j < k) v = (float)((AX[i * ldax + j] - theta[j] * X[i * ldx + j]) * inv_s[j]);
+    R[i * ldr + j] = v;
+  }
+}
+
+// Y[i, j] = pt[j] X[i, j] + sd[j] Z[i, j] (FP64 result from the FP32 correction block).
+__global__ void combine_kernel(int64_t n, int64_t k, const double *__restrict__ X, int64_t ldx,
+                               const float *__restrict__ Z, int64_t ldz,
+                               const double *__restrict__ pt, const double *__restrict__ sd,
+                               double *__restrict__ Y, int64_t ldy) {
+  const int64_t total = n * k;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t / k, j = t % k;
+    Y[i * ldy + j] = pt[j] * X[i * ldx + j] + sd[j] * (double)Z[i * ldz + j];
+  }
+}
+
+// out = crow[j] Q + alpha AX + beta B1 - B2 (per-column coefficient; operators without a
+// fused step: the model stencils and half storage).
+template <typename T>
+__global__ void percol_axpy_kernel(int64_t n, int64_t b, const T *__restrict__ Q,
+                                   const T *__restrict__ AX, const T *__restrict__ B1,
+                                   const T *__restrict__ B2, T *__restrict__ out, int64_t ld,
+                                   const T *__restrict__ crow, T alpha, T beta) {
+  const int64_t total = n * b;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t / b, j = t % b;
+    const int64_t e = i * ld + j;
+    out[e] = crow[j] * Q[e] + alpha * AX[e] + beta * B1[e] - B2[e];
+  }
+}
+
+int grid_of(int64_t total) {
+  const int64_t g = (total + 255) / 256;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
+}
+
+}  // namespace
+
+// Y = q(A_hat) Q where column j of the n x b blocks (ld = b) runs its own polynomial with
+// coefficients coef[m * b + j], m = 0..K (row-major (K+1) x b table, FP32 or FP64 like
+// the blocks).  colseg is the identity map 0..b-1 on the device; B1, B2, TMP (and AX for
+// operators without a fused step) are n x b work blocks.  The recurrence starts from zero
+// blocks, so its first product multiplies zeros (one extra step out of K+1).
+template <typename T>
+FilterCount percol_filter(const sma_op *op, cudaStream_t st, const T *coef, int64_t K,
+                          double smin, double smax, const T *Q, T *Y, int64_t b,
+                          const int *colseg, T *B1, T *B2, T *TMP, T *AX) {
+  FilterCount fc;
+  const int64_t n = op->n;
+  require(op->kind != OP_MATBLOCK, SMA_ERR_ARG, "the per-column filter needs a device operator");
+  const double c = 0.5 * (smin + smax), invd = 2.0 / (smax - smin);
+  const double alpha = 2.0 * invd, beta = -2.0 * c * invd;
+  const size_t bytes = (size_t)(n * b) * sizeof(T);
+  SMA_CUDA(cudaMemsetAsync(B1, 0, bytes, st));
+  SMA_CUDA(cudaMemsetAsync(B2, 0, bytes, st));
+  const bool fused = op->kind == OP_CSR;
+  auto step = [&](const T *crow, T *out, double al, double be) {
+    if (fused) {
+      csr_clenshaw_step_seg<T>(op, st, b, Q, b, B1, B2, b, out, b, crow, colseg, al, be, true);
+    } else {
+      if (op->kind == OP_CSR_HALF)
+        half_product<T>(op, st, B1, b, AX, b, b);
+      else
+        launch_clenshaw_step<T>(op, st, b, nullptr, 0, B1, nullptr, b, AX, b, 0.0, 1.0, 0.0, false);
+      percol_axpy_kernel<T><<<grid_of(n * b), 256, 0, st>>>(n, b, Q, AX, B1, B2, out, b, crow,
+                                                           (T)al, (T)be);
+      SMA_CHECK_LAUNCH();
+    }
+  };
+  const double mat_bytes = clenshaw_step_bytes(op, 0, sizeof(T));
+  const double blk = (double)n * (double)b * sizeof(T);
+  for (int64_t k = K; k >= 1; --k) {
+    step(coef + k * b, TMP, alpha, beta);
+    T *t = B2;  // B1, B2, TMP = TMP, B1, B2
+    B2 = B1;
+    B1 = TMP;
+    TMP = t;
+  }
+  step(coef, Y, invd, -(c * invd));
+  fc.steps = K + 1;
+  fc.bytes = (double)(K + 1) * (mat_bytes + 4 * blk);
+  return fc;
+}
+
+template FilterCount percol_filter<float>(const sma_op *, cudaStream_t, const float *, int64_t,
+                                          double, double, const float *, float *, int64_t,
+                                          const int *, float *, float *, float *, float *);
+template FilterCount percol_filter<double>(const sma_op *, cudaStream_t, const double *, int64_t,
+                                           double, double, const double *, double *, int64_t,
+                                           const int *, double *, double *, double *, double *);
+
+// Coefficients e_0..e_{K-1} of q_t (p's divided difference at t) and p(t), from the
+// Clenshaw intermediates of p at t.
+void divided_difference(const std::vector<double> &c, double t, double *e, double *pt) {
+  const int64_t K = (int64_t)c.size() - 1;
+  double b1 = 0.0, b2 = 0.0;  // b_{m+1}, b_{m+2}
+  for (int64_t m = K; m >= 1; --m) {
+    const double bm = c[m] + 2.0 * t * b1 - b2;
+    if (m >= 2) e[m - 1] = 2.0 * bm;
+    else e[0] = bm;
+    b2 = b1;
+    b1 = bm;
+  }
+  *pt = c[0] + t * b1 - b2;
+}
+
+using detail::dev_to_host;
+
+PolishOut polish_mixed(const sma_op *op, const std::vector<double> &coeffs, double smin,
+                       double smax, double *X, int64_t k, const PolishDone &done,
+                       int64_t max_passes, FilterCount &fc, int64_t *qr_fallbacks) {
+  PolishOut out;
+  sma_ctx *ctx = op->ctx;
+  cudaStream_t st = ctx->stream;
+  const int64_t n = op->n;
+  const int64_t K = (int64_t)coeffs.size() - 1;
+  require(K >= 1, SMA_ERR_ARG, "the polish needs a filter of degree >= 1");
+  const double c = 0.5 * (smin + smax), d = 0.5 * (smax - smin);
+  const int64_t kpad = (k + 7) / 8 * 8;  // FP32 rows of 32-byte multiples: full vector width
+  Dense dn(ctx);
+  DevBuf<double> AX(n * k, st), Y(n * k, st), H(k * k, st), mu(k, st), lam_d(k, st), res_d(k, st),
+      scratch, theta_d(k, st), inv_s_d(k, st), pt_d(k, st), sd_d(k, st);
+  DevBuf<float> R32(n * kpad, st), Z32(n * kpad, st), B1(n * kpad, st), B2(n * kpad, st),
+      TMP(n * kpad, st), AX32, coef32(K * kpad, st);
+  if (op->kind != OP_CSR) AX32.alloc(n * kpad, st);
+  DevBuf<int> colseg(kpad, st);
+  {
+    std::vector<int> idn(kpad);
+    for (int64_t j = 0; j < kpad; ++j) idn[j] = (int)j;
+    SMA_CUDA(cudaMemcpyAsync(colseg.p, idn.data(), kpad * sizeof(int), cudaMemcpyHostToDevice, st));
+    SMA_CUDA(cudaStreamSynchronize(st));
+  }
+  // Rayleigh-Ritz with A on span(V) (V n x k, orthonormalized in place): X = V E,
+  // out.lam/out.res its Ritz values (ascending) and residual norms.
+  auto rayleigh_ritz = [&](double *V) {
+    orthonormalize(ctx, n, k, V, k, false, 0.0, nullptr, qr_fallbacks);
+    op_apply(op, st, V, k, AX.p, k, k);
+    dn.gram(n, k, k, V, k, AX.p, k, H.p, k);
+    dn.syevd(k, H.p, k, mu.p, true);
+    dn.mul_small(n, k, k, V, k, H.p, k, X, k, 1.0, 0.0);
+    op_apply(op, st, X, k, AX.p, k, k);
+    column_reduce(st, 0, n, k, X, k, AX.p, k, nullptr, lam_d.p, scratch);
+    column_reduce(st, 1, n, k, X, k, AX.p, k, lam_d.p, res_d.p, scratch);
+    out.lam = dev_to_host(st, lam_d.p, k);
+    out.res = dev_to_host(st, res_d.p, k);
+  };
+  // consistent start: Rayleigh-Ritz on the candidates themselves
+  SMA_CUDA(cudaMemcpyAsync(Y.p, X, n * k * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  rayleigh_ritz(Y.p);
+  std::vector<double> ch(K * kpad), inv_s(k), pt(k), sd(k);
+  std::vector<float> cf(K * kpad, 0.f);
+  std::vector<double> e(K);
+  for (int64_t pass = 0; pass < max_passes && !done(out.lam, out.res); ++pass) {
+    for (int64_t j = 0; j < k; ++j) {
+      const double s = out.res[j];
+      inv_s[j] = s > 0.0 ? 1.0 / s : 0.0;
+      sd[j] = s / d;
+      divided_difference(coeffs, (out.lam[j] - c) / d, e.data(), &pt[j]);
+      for (int64_t m = 0; m < K; ++m) cf[m * kpad + j] = (float)e[m];
+    }
+    SMA_CUDA(cudaMemcpyAsync(theta_d.p, out.lam.data(), k * sizeof(double), cudaMemcpyHostToDevice, st));
+    SMA_CUDA(cudaMemcpyAsync(inv_s_d.p, inv_s.data(), k * sizeof(double), cudaMemcpyHostToDevice, st));
+    SMA_CUDA(cudaMemcpyAsync(pt_d.p, pt.data(), k * sizeof(double), cudaMemcpyHostToDevice, st));
+    SMA_CUDA(cudaMemcpyAsync(sd_d.p, sd.data(), k * sizeof(double), cudaMemcpyHostToDevice, st));
+    SMA_CUDA(cudaMemcpyAsync(coef32.p, cf.data(), cf.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    residual_f32_kernel<<<grid_of(n * kpad), 256, 0, st>>>(n, k, kpad, X, k, AX.p, k, theta_d.p,
+                                                          inv_s_d.p, R32.p, kpad);
+    SMA_CHECK_LAUNCH();
+    const FilterCount f = percol_filter<float>(op, st, coef32.p, K - 1, smin, smax, R32.p, Z32.p,
+                                               kpad, colseg.p, B1.p, B2.p, TMP.p, AX32.p);
+    fc.steps += f.steps;
+    fc.bytes += f.bytes;
+    combine_kernel<<<grid_of(n * k), 256, 0, st>>>(n, k, X, k, Z32.p, kpad, pt_d.p, sd_d.p, Y.p, k);
+    SMA_CHECK_LAUNCH();
+    rayleigh_ritz(Y.p);
+    SMA_CUDA(cudaStreamSynchronize(st));  // the host tables above are rewritten next pass
+    out.passes += 1;
+  }
+  return out;
+}
+
+}  // namespace sma

@@ -7,6 +7,7 @@
 #include <cusolverDn.h>
 
 #include <atomic>
+#include <functional>
 #include <cstdint>
 #include <cstdio>
 #include <map>
@@ -97,6 +98,9 @@ struct sma_ctx {
   bool filter_graphs = true;
   // SMA_PERSISTENT=1: CSR filters run as one persistent cooperative launch (persistent.cu)
   bool persistent = false;
+  // SMA_CUBLAS_DENSE=1: the tall-skinny products go through cuBLAS DGEMM instead of this
+  // library's DMMA kernels (dgemm.cu) -- for comparisons
+  bool cublas_dense = false;
 };
 
 // OP_CSR_HALF: the upper triangle of a symmetric matrix only (half.cu)
@@ -191,12 +195,12 @@ template <typename T>
 void csr_clenshaw_step_untuned(const sma_op *op, cudaStream_t st, int64_t b, const T *Q,
                                int64_t ldq, const T *B1, const T *B2, int64_t ldb, T *out,
                                int64_t ldo, double ck, double alpha, double beta, bool has_self);
-// The segmented CSR step of batched slicing: column c uses the coefficient
-// cseg[colseg8[c / 8]] (csr_clenshaw.cuh).
+// The segmented CSR step (batched slicing, the POLFED polish): column c uses the
+// coefficient cseg[colseg[c]] (csr_clenshaw.cuh).
 template <typename T>
 void csr_clenshaw_step_seg(const sma_op *op, cudaStream_t st, int64_t b, const T *Q, int64_t ldq,
                            const T *B1, const T *B2, int64_t ldb, T *out, int64_t ldo,
-                           const T *cseg, const int *colseg8, double alpha, double beta,
+                           const T *cseg, const int *colseg, double alpha, double beta,
                            bool tuned);
 // out = ck * Q
 template <typename T>
@@ -248,6 +252,8 @@ int check_csr_device(const sma_op *op);
 void launch_add_diagonal(cudaStream_t st, int64_t k, double *G, int64_t ld, double shift);
 // Zero the strict lower triangle of a k x k column-major matrix
 void launch_zero_lower(cudaStream_t st, int64_t k, double *G, int64_t ld);
+// I (k x k, column-major, ld)
+void launch_identity(cudaStream_t st, int64_t k, double *G, int64_t ld);
 
 // ------------------------------------------------------------------ KPM (kpm.cu)
 void kpm_moments(const sma_op *op, int64_t M, int64_t R, uint64_t seed, double smin,
@@ -324,8 +330,22 @@ void op_apply(const sma_op *op, cudaStream_t st, const double *X, int64_t ldx, d
 double clenshaw_step_bytes(const sma_op *op, int64_t b, int elem_bytes);
 
 // ------------------------------------------------------------------ dense (dense.cu)
+// FP64 tensor-core products of this library (dgemm.cu).
+// Y (n x p, row-major) = alpha X B + beta Y, X n x m row-major, B = C (m x p column-major,
+// ldc) or B = C^T (transC; C p x m column-major).  In place over X allowed when p <= 64 and
+// beta = 0.
+void dgemm_update(cudaStream_t st, int num_sms, int64_t n, int64_t m, int64_t p, const double *X,
+                  int64_t ldx, const double *C, int64_t ldc, bool transC, double *Y, int64_t ldy,
+                  double alpha, double beta);
+// C (m x k, column-major, ldc) = alpha X^T Y + beta C; deterministic split-n reduction
+// through `work` (grown as needed).
+void dgemm_gram(cudaStream_t st, int num_sms, int64_t n, int64_t m, int64_t k, const double *X,
+                int64_t ldx, const double *Y, int64_t ldy, double *C, int64_t ldc, double alpha,
+                double beta, DevBuf<double> &work);
+
 struct Dense {
   sma_ctx *ctx;
+  DevBuf<double> work;  // split-n partial products of gram()
   explicit Dense(sma_ctx *c) : ctx(c) {}
   // C (col-major, m x k, ldc) = alpha * X^T Y + beta*C, X row-major n x m (ldx), Y n x k
   void gram(int64_t n, int64_t m, int64_t k, const double *X, int64_t ldx, const double *Y,
@@ -345,6 +365,28 @@ struct Dense {
 int64_t orthonormalize(sma_ctx *ctx, int64_t n, int64_t k, double *X, int64_t ldx,
                        bool truncate, double rtol, std::vector<double> *R_out,
                        int64_t *fallbacks);
+
+// ------------------------------------------------------------------ polish (polish.cu)
+// Y = q(A_hat) Q with a polynomial per column: coef[m * b + j] is coefficient m of column
+// j (m = 0..K), blocks n x b row-major with ld = b, colseg the identity map on the device.
+template <typename T>
+FilterCount percol_filter(const sma_op *op, cudaStream_t st, const T *coef, int64_t K,
+                          double smin, double smax, const T *Q, T *Y, int64_t b,
+                          const int *colseg, T *B1, T *B2, T *TMP, T *AX);
+// e[0..K-1]: Chebyshev coefficients of (p(s) - p(t)) / (s - t) for p = sum c_m T_m; *pt = p(t).
+void divided_difference(const std::vector<double> &c, double t, double *e, double *pt);
+struct PolishOut {
+  std::vector<double> lam, res;  // Ritz values (ascending) and residual norms of X
+  int64_t passes = 0;
+};
+// done(lam, res) ends the passes early.
+using PolishDone = std::function<bool(const std::vector<double> &, const std::vector<double> &)>;
+// Rayleigh-Ritz with A on the k columns of X (n x k, ld k, FP64, in place), then up to
+// max_passes filtered subspace iterations with p = sum coeffs[m] T_m(A_hat), each applying
+// p as p(theta) x + q_theta(A_hat) r / d with q in FP32; X ends as the last Ritz vectors.
+PolishOut polish_mixed(const sma_op *op, const std::vector<double> &coeffs, double smin,
+                       double smax, double *X, int64_t k, const PolishDone &done,
+                       int64_t max_passes, FilterCount &fc, int64_t *qr_fallbacks);
 
 // ------------------------------------------------------------------ result
 }  // namespace sma

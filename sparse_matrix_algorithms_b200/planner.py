@@ -366,12 +366,15 @@ def _polfed_good(lam, res, emin, emax, nrm):
 
 def solve_polfed_window(A, window, planner: Optional[WindowPlanner] = None, *, s: int = 8,
                         smin=None, smax=None, mu=None, seed: int = 1,
-                        report: Optional[dict] = None, stats: Optional[dict] = None):
+                        report: Optional[dict] = None, stats: Optional[dict] = None,
+                        precision: str = "fp64", vectors: bool = True):
     """POLFED on one window with a planned (nev, degree, mmax): the learned plan when a
     planner is given, else the plain rule.  A learned plan that returns fewer than
     0.85 N - 3 converged in-window pairs (N the KPM count) is redone with the plain rule.
     Returns ``(lam, X, res)``; ``report`` receives the plans, the column-steps spent and
-    whether the window was redone; ``stats`` the solver statistics of the last POLFED run."""
+    whether the window was redone; ``stats`` the solver statistics of the last POLFED run.
+    ``precision`` is the filter arithmetic of both runs (``"mixed"``: FP32 basis, FP64
+    polish); ``vectors=False`` keeps the eigenvectors on the device (X is None)."""
     from .api import polfed
 
     op = _op_of(A)
@@ -392,7 +395,8 @@ def solve_polfed_window(A, window, planner: Optional[WindowPlanner] = None, *, s
 
     def run(nev, K, mmax):
         return polfed(op, nev, K, s=s, smin=smin, smax=smax, sigma=0.5 * (a + b), emin=a,
-                      emax=b, window_type="delta", mmax=mmax, seed=seed, stats=stats)
+                      emax=b, window_type="delta", mmax=mmax, seed=seed, stats=stats,
+                      precision=precision, vectors=vectors)
 
     lam, X, res = run(*plan)
     cost = polfed_cost(plan[1], plan[2], s)
@@ -405,6 +409,99 @@ def solve_polfed_window(A, window, planner: Optional[WindowPlanner] = None, *, s
         report.update(dict(plan=plan, plain=(nev0, K0, m0), cost=cost, redone=redone,
                            kpm_count=N, good=_polfed_good(lam, res, a, b, nrm)))
     return lam, X, res
+
+
+def plan_polfed_windows(A, windows, planner: Optional[WindowPlanner], *, s: int, smin: float,
+                        smax: float, mu: np.ndarray):
+    """Per window: the KPM count N, the plain rule's (nev, degree, mmax) and the plan --
+    the network's when a planner is given, else the plain rule."""
+    op = _op_of(A)
+    counts, plain, plans = [], [], []
+    feats = []
+    for a, b in windows:
+        N = kpm_count(mu, op.n, smin, smax, a, b)
+        K0, m0 = polfed_plain_rule(N, smin, smax, a, b, s)
+        counts.append(N)
+        plain.append((polfed_nev(N), K0, m0))
+        feats.append(window_features(mu, smin, smax, a, b))
+    if planner is None:
+        return counts, plain, list(plain)
+    Y = np.clip(planner.forward(np.stack(feats)), *_CLIP)
+    for (nev0, K0, m0), N, y in zip(plain, counts, Y):
+        plans.append((max(nev0, polfed_nev(N * math.exp(y[2]))),
+                      max(1, int(round(K0 * math.exp(y[0])))),
+                      max(2, int(math.ceil(m0 * math.exp(y[1]))))))
+    return counts, plain, plans
+
+
+def solve_polfed_windows(A, windows, planner: Optional[WindowPlanner] = None, *, s: int = 8,
+                         smin=None, smax=None, mu=None, seed: int = 1,
+                         precision: str = "fp64", report: Optional[dict] = None,
+                         stats: Optional[dict] = None, vectors: bool = True):
+    """Batched POLFED over ``windows`` with a planned (nev, degree, mmax) per window (the
+    learned plan when a planner is given, else the plain rule), all windows in one
+    :func:`polfed_windows` call.  Every window whose learned plan returns fewer than
+    0.85 N - 3 converged in-window pairs (N its KPM count) is solved again with the plain
+    rule (the redone windows batched together).  Returns ``(lam, X, res, win)``;
+    ``report`` receives the plans, the plain rule, the column-steps spent and the windows
+    redone."""
+    from .api import polfed_windows
+
+    op = _op_of(A)
+    if smin is None or smax is None:
+        smin, smax = op.gershgorin_bounds()
+    if mu is None:
+        mu = kpm_moments(op, N_MOMENTS, 16, smin=smin, smax=smax)
+    windows = [tuple(map(float, w)) for w in windows]
+    nrm = max(abs(smin), abs(smax))
+    counts, plain, plans = plan_polfed_windows(op, windows, planner, s=s, smin=smin, smax=smax,
+                                               mu=mu)
+
+    def run(ws, pl, st):
+        return polfed_windows(op, [windows[w] for w in ws], [p[0] for p in pl], [p[1] for p in pl],
+                              [p[2] for p in pl], s=s, smin=smin, smax=smax, window_type="delta",
+                              seed=seed, precision=precision, stats=st, vectors=vectors)
+
+    ids = list(range(len(windows)))
+    lam, X, res, win = run(ids, plans, stats)
+    cost = [polfed_cost(p[1], p[2], s) for p in plans]
+    redo = []
+    if planner is not None:
+        for w in ids:
+            a, b = windows[w]
+            sel = win == w
+            if _polfed_good(lam[sel], res[sel], a, b, nrm) < 0.85 * counts[w] - 3:
+                redo.append(w)
+    if redo:
+        st2 = {}
+        l2, X2, r2, w2 = run(redo, [plain[w] for w in redo], st2)
+        keep = ~np.isin(win, redo)
+        parts_l, parts_r, parts_w = [lam[keep]], [res[keep]], [win[keep]]
+        parts_x = [X[:, keep]] if X is not None else []
+        for j, w in enumerate(redo):
+            sel = w2 == j
+            parts_l.append(l2[sel])
+            parts_r.append(r2[sel])
+            parts_w.append(np.full(int(sel.sum()), w))
+            if X2 is not None:
+                parts_x.append(X2[:, sel])
+            cost[w] += polfed_cost(plain[w][1], plain[w][2], s)
+        order_w = np.concatenate(parts_w)
+        perm = np.argsort(order_w, kind="stable")
+        lam = np.concatenate(parts_l)[perm]
+        res = np.concatenate(parts_r)[perm]
+        win = order_w[perm]
+        X = np.concatenate(parts_x, axis=1)[:, perm] if parts_x else None
+        if stats is not None:
+            for key in ("filter_ms", "orth_ms", "rr_ms", "filter_bytes", "spmm_steps",
+                        "spmm_columns", "kernel_launches", "polish_iterations"):
+                if key in st2:
+                    stats[key] = stats.get(key, 0) + st2[key]
+    if report is not None:
+        report.update(dict(plan=plans, plain=plain, cost=cost, redone=redo, kpm_count=counts,
+                           good=[_polfed_good(lam[win == w], res[win == w], *windows[w], nrm)
+                                 for w in ids]))
+    return lam, X, res, win
 
 
 def polfed_training_rows(A, windows, *, s: int = 8, smin=None, smax=None, mu=None,

@@ -1,0 +1,95 @@
+"""Parity at the benchmark's own configurations, arm by arm, exactly as ``bench.py`` runs
+them (its ``arm_*`` functions on its ``Workload``):
+
+* C2 -- XXZ L=18 (n=48620), h=5, seed 1, the 200 eigenvalues nearest the spectral centre,
+  s=32 -- against the dense FP64 spectrum (tests/golden/xxz_L18_spectrum.npz): the count in
+  the window exact, every eigenvalue within 1e-12 ||A|| of its dense counterpart, every
+  relative residual ||Ax - lam x|| / ||A|| <= 1e-10 (the reference's own checks,
+  chebyshev_subspace_iteration.jl:905-979, and its return rule, polfed.jl:1148-1157);
+* C3 -- 3D Anderson L=64 (n=262144), W=16.5, seed 2, the KPM-placed 500-eigenvalue window
+  -- against the Sylvester-inertia count 494 (tests/golden/anderson_L64_inertia.json), with
+  relative residuals <= 1e-10 recomputed on the host from the returned vectors, and the
+  arms' eigenvalues agreeing with each other to 1e-12 ||A|| (no dense spectrum exists at
+  this size).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def c2(lib_built):
+    import bench
+    import sparse_matrix_algorithms_b200 as S
+
+    wl = bench.Workload("c2")
+    return wl, S.SparseOperator(wl.A)
+
+
+@pytest.fixture(scope="module")
+def c3(lib_built):
+    import bench
+    import sparse_matrix_algorithms_b200 as S
+
+    wl = bench.Workload("c3")
+    op = S.SparseOperator(wl.A)
+    lo, hi = S.lanczos_bounds(op, steps=bench.LANCZOS_STEPS)
+    wl.norm = max(abs(lo), abs(hi))
+    return wl, op
+
+
+@pytest.fixture(scope="module")
+def planner_net(lib_built):
+    from sparse_matrix_algorithms_b200 import planner as P
+
+    return P.WindowPlanner.load(P.POLFED_WEIGHTS)
+
+
+def _run(arm, wl, op, net, precision):
+    import bench
+
+    if arm == "plain":
+        return bench.arm_plain(wl, op, vectors=True)
+    if arm == "tuned":
+        return bench.arm_tuned(wl, op, vectors=True)
+    return bench.arm_pipeline(wl, op, net, precision, vectors=True)
+
+
+def _host_residuals(A, X, lam):
+    return np.linalg.norm(A @ X - X * lam, axis=0)
+
+
+@pytest.mark.parametrize("arm,precision", [("plain", "fp64"), ("tuned", "fp64"),
+                                           ("pipeline", "fp64"), ("pipeline", "mixed")])
+def test_c2_against_dense_spectrum(c2, planner_net, arm, precision):
+    wl, op = c2
+    lam, X, res = _run(arm, wl, op, planner_net, precision)
+    inside = (lam >= wl.emin) & (lam <= wl.emax)
+    assert int(inside.sum()) == wl.exact_count == 200
+    got = np.sort(lam[inside])
+    assert np.abs(got - wl.exact).max() <= 1e-12 * wl.norm
+    assert res[inside].max() <= 1e-10 * wl.norm
+    r = _host_residuals(wl.A, X[:, inside], lam[inside])
+    assert r.max() <= 1e-10 * wl.norm
+    assert np.abs(r - res[inside]).max() <= 1e-12 * wl.norm
+
+
+_C3_LAMBDA = {}
+
+
+@pytest.mark.parametrize("arm,precision", [("tuned", "fp64"), ("pipeline", "fp64"),
+                                           ("pipeline", "mixed")])
+def test_c3_inertia_count_and_residuals(c3, planner_net, arm, precision):
+    wl, op = c3
+    lam, X, res = _run(arm, wl, op, planner_net, precision)
+    inside = (lam >= wl.emin) & (lam <= wl.emax)
+    assert int(inside.sum()) == wl.exact_count == 494
+    assert res[inside].max() <= 1e-10 * wl.norm
+    r = _host_residuals(wl.A, X[:, inside], lam[inside])
+    assert r.max() <= 1e-10 * wl.norm
+    got = np.sort(lam[inside])
+    assert np.all(np.diff(got) > 0)  # distinct: no eigenvalue returned twice
+    for other in _C3_LAMBDA.values():  # every arm finds the same 494 eigenvalues
+        assert np.abs(got - other).max() <= 1e-12 * wl.norm
+    _C3_LAMBDA[(arm, precision)] = got

@@ -63,7 +63,7 @@ def test_persistent_polfed_and_chebyshev_bit_identical(lib_built, monkeypatch):
 
 def test_bounded_barrier_reports_timeout_and_context_survives(lib_built):
     """Failure detection without a fault: the grid barrier waits for a CTA that was never
-    launched, gives up after its spin limit (~10 ms), sets the error flag and returns; the
+    launched, gives up after its wait limit (10 ms of elapsed time), sets the error flag and returns; the
     host reads SMA_ERR_TIMEOUT and the context keeps working."""
     import ctypes
 

@@ -60,24 +60,48 @@ def test_noalloc_filter_matches_regular_entry_on_two_calls(lib_built):
         assert np.all(Y[:, b:] == 3.0)  # columns beyond b untouched
 
 
-def test_noalloc_filter_stencil_operator_and_size_limit(lib_built):
+@pytest.mark.parametrize("stencil", ["lap1d", "anderson", "xxz"])
+def test_noalloc_filter_stencil_operators(lib_built, stencil):
+    """Every model stencil the entry point accepts: 1D Laplacian, Anderson, XXZ."""
+    import torch
+    import sparse_matrix_algorithms_b200 as S
+
+    if stencil == "lap1d":
+        op, smin, smax = S.Lap1dOperator(5000), 0.0, 4.0
+    elif stencil == "anderson":
+        op = S.AndersonOperator(12, 16.5, 5)
+        smin, smax = O.gershgorin_bounds(M.anderson3d(12, 16.5, 5))
+    else:
+        op = S.XXZOperator(12, 5.0, 1)
+        smin, smax = O.gershgorin_bounds(M.xxz_sz0(12, 5.0, 1))
+    n, b = op.n, 16
+    mid = 0.5 * (smin + smax)
+    c = np.ascontiguousarray(O.build_coeffs(80, smin, smax, mid, mid - 0.1, mid + 0.1, "delta", True))
+    Q = torch.as_tensor(M.splitmix_normal(3, n, b), device="cuda").contiguous()
+    for _ in range(2):
+        Yref = _run("sma_apply_poly_block_dev", op, c, smin, smax, Q, b,
+                    torch.empty((n, b), dtype=torch.float64, device="cuda"), b, b)
+        Y = _run("sma_apply_poly_block_noalloc", op, c, smin, smax, Q, b,
+                 torch.empty((n, b), dtype=torch.float64, device="cuda"), b, b)
+        assert np.abs(Y - Yref).max() <= 1e-12 * max(1.0, np.abs(Yref).max())
+
+
+def test_noalloc_filter_size_limit(lib_built):
     import torch
     import sparse_matrix_algorithms_b200 as S
     from sparse_matrix_algorithms_b200 import _lib as L
 
-    n, b = 5000, 16
-    op = S.Lap1dOperator(n)
+    b = 16
     c = np.ascontiguousarray(O.build_coeffs(80, 0.0, 4.0, 2.0, 1.9, 2.1, "delta", True))
-    Q = torch.as_tensor(M.splitmix_normal(3, n, b), device="cuda").contiguous()
-    for _ in range(2):
-        Yref = _run("sma_apply_poly_block_dev", op, c, 0.0, 4.0, Q, b,
-                    torch.empty((n, b), dtype=torch.float64, device="cuda"), b, b)
-        Y = _run("sma_apply_poly_block_noalloc", op, c, 0.0, 4.0, Q, b,
-                 torch.empty((n, b), dtype=torch.float64, device="cuda"), b, b)
-        assert np.abs(Y - Yref).max() <= 1e-12 * max(1.0, np.abs(Yref).max())
+    Q = torch.zeros((4, b), dtype=torch.float64, device="cuda")
     # n*b beyond the 2,097,152-element capacity is rejected before any launch
     big = S.Lap1dOperator(300_000)
     rc = L.load().sma_apply_poly_block_noalloc(big.handle, c.ctypes.data, len(c) - 1, 0.0, 4.0,
                                                Q.data_ptr(), b, Q.data_ptr(), b, b)
     assert rc == L.SMA_ERR_ARG
     assert b"capacity" in L.load().sma_last_error()
+    # half storage needs an extra product block, so it is refused rather than allocated
+    half = S.SparseOperator(M.lap1d(64), storage="upper")
+    rc = L.load().sma_apply_poly_block_noalloc(half.handle, c.ctypes.data, len(c) - 1, 0.0, 4.0,
+                                               Q.data_ptr(), b, Q.data_ptr(), b, b)
+    assert rc == L.SMA_ERR_ARG
