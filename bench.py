@@ -187,22 +187,24 @@ def arm_tuned(wl, op, stats=None, vectors=False):
 
 def arm_pipeline(wl, op, net, precision="mixed", stats=None, report=None, vectors=False):
     """The untuned pipeline: Lanczos bounds, KPM moments, the learned plan with the plain
-    rule as fallback, in the given filter arithmetic."""
+    rule as fallback, batched POLFED (here over the workload's one window) in the given
+    filter arithmetic."""
     import sparse_matrix_algorithms_b200 as S
     from sparse_matrix_algorithms_b200 import planner as P
 
     lo, hi = S.lanczos_bounds(op, steps=LANCZOS_STEPS)
     mu = S.kpm_moments(op, P.N_MOMENTS, 16, smin=lo, smax=hi)
     rep = {}
-    out = P.solve_polfed_window(op, (wl.emin, wl.emax), net, s=wl.s, smin=lo, smax=hi, mu=mu,
-                                report=rep, stats=stats, precision=precision, vectors=vectors)
+    lam, X, res, _ = P.solve_polfed_windows(op, [(wl.emin, wl.emax)], net, s=wl.s, smin=lo,
+                                            smax=hi, mu=mu, report=rep, stats=stats,
+                                            precision=precision, vectors=vectors)
     if stats is not None:
-        stats["plan"] = list(rep["plan"])
-        stats["plain_rule"] = list(rep["plain"])
-        stats["redone"] = rep["redone"]
+        stats["plan"] = list(rep["plan"][0])
+        stats["plain_rule"] = list(rep["plain"][0])
+        stats["redone"] = bool(rep["redone"])
     if report is not None:
         report.update(rep)
-    return out
+    return lam, X, res
 
 
 class ClockSampler:
@@ -536,6 +538,120 @@ TRAFFIC = {
 }
 
 
+def multi_workload(name):
+    """C4 / C5: the matrix and its windows, placed from KPM moments (256 moments, 32
+    Rademacher vectors, seed 11) on 100-step Lanczos bounds, computed at set-up.
+
+    C4  XXZ L=20 Sz=0 (n=184756), h=3, seed 3: 16 contiguous windows centred at E=0 whose
+        KPM counts are uneven, 50..400 (seeded); the 16 windows the configuration names as
+        tiling [-2, 2] would each hold thousands of eigenvalues ([-2, 2] holds ~6e4), so the
+        counts are kept and the windows placed contiguously around E=0 instead.
+    C5  3D Anderson L=96 (n=884736), W=12, seed 4: one window of 1000 KPM-estimated
+        eigenvalues centred at E=0."""
+    import sparse_matrix_algorithms_b200 as S
+    from sparse_matrix_algorithms_b200 import matrices as M
+    from sparse_matrix_algorithms_b200 import planner as P
+
+    if name == "c4":
+        A = M.config_matrix("xxz_L20")
+        counts = [float(np.round(50 + 350 * x)) for x in M.splitmix_uniform(3, 16)]
+        s = 32
+        text = ("C4 batched POLFED: XXZ L=20 Sz=0 (n=184756), h~U[-3,3] seed 3; 16 contiguous "
+                "KPM-placed windows around E=0 with uneven counts 50..400; s=32")
+    elif name == "c5":
+        A = M.config_matrix("anderson_L96")
+        counts = [1000.0]
+        s = 64
+        text = ("C5 POLFED: 3D Anderson L=96 (n=884736), W=12, seed 4; 1000 KPM-placed "
+                "eigenvalues centred at E=0; s=64")
+    else:
+        raise ValueError(name)
+    op = S.SparseOperator(A)
+    lo, hi = S.lanczos_bounds(op, steps=LANCZOS_STEPS)
+    mu = S.kpm_moments(op, P.N_MOMENTS, 32, smin=lo, smax=hi, seed=11)
+    wins = P.windows_by_count(mu, A.shape[0], lo, hi, 0.0, counts)
+    return A, op, wins, counts, s, (lo, hi), text
+
+
+def run_multi(args):
+    """C4 or C5 (one solve per arm, builder measurements): the pipeline -- Lanczos bounds,
+    KPM moments, the learned plan per window, batched MIXED POLFED over all windows, the
+    plain rule as fallback -- against the plain FP64 GPU path, one polfed call per window
+    (Gershgorin bounds, Jackson-damped delta window, degree 12 d / width, mmax 2.8 N / s).
+    Pairs count inside their windows at relative residual <= 1e-10; the two arms'
+    eigenvalues are compared window by window."""
+    import torch
+
+    import sparse_matrix_algorithms_b200 as S
+    from sparse_matrix_algorithms_b200 import planner as P
+
+    torch.cuda.set_device(0)
+    A, op, wins, counts, s, (lo, hi), text = multi_workload(args.workload)
+    net = P.WindowPlanner.load(P.POLFED_WEIGHTS)
+    stream = torch.cuda.ExternalStream(S.context(0).stream, device=0)
+    norm = max(abs(lo), abs(hi))
+    out = {"workload": text, "windows": wins, "kpm_counts": counts}
+
+    def good(lam, res, win):
+        return [int(np.sum((lam[win == w] >= a) & (lam[win == w] <= b) & (res[win == w] <= 1e-10 * norm)))
+                for w, (a, b) in enumerate(wins)]
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return r, e0.elapsed_time(e1) / 1e3
+
+    def pipeline():
+        l2, h2 = S.lanczos_bounds(op, steps=LANCZOS_STEPS)
+        mu = S.kpm_moments(op, P.N_MOMENTS, 16, smin=l2, smax=h2)
+        rep, st = {}, {}
+        r = P.solve_polfed_windows(op, wins, net, s=s, smin=l2, smax=h2, mu=mu,
+                                   precision=args.precision, report=rep, stats=st, vectors=False)
+        return r, rep, st
+
+    ((lam, _, res, win), rep, st), t_pipe = timed(pipeline)
+    g_pipe = good(lam, res, win)
+    out["pipeline"] = {"seconds": t_pipe, "pairs": int(sum(g_pipe)), "per_window": g_pipe,
+                       "eigenpairs_per_s": sum(g_pipe) / t_pipe, "plans": rep["plan"],
+                       "plain_rule": rep["plain"], "redone": rep["redone"],
+                       "filter_ms": st.get("filter_ms"), "orth_ms": st.get("orth_ms"),
+                       "rr_ms": st.get("rr_ms"), "polish_passes": st.get("polish_iterations"),
+                       "spmm_gbs": st["filter_bytes"] / st["filter_ms"] / 1e6 if st.get("filter_ms") else None}
+    print(json.dumps(out), flush=True)
+    if args.no_plain:
+        return
+    gl, gh = op.gershgorin_bounds()
+    mu_g = S.kpm_moments(op, P.N_MOMENTS, 16, smin=gl, smax=gh)
+
+    def plain():
+        res_all = []
+        for (a, b) in wins:
+            N = S.kpm_count(mu_g, op.n, gl, gh, a, b)
+            K, mm = P.polfed_plain_rule(N, gl, gh, a, b, s)
+            res_all.append(S.polfed(op, P.polfed_nev(N), K, s=s, smin=gl, smax=gh, sigma=0.5 * (a + b),
+                                    emin=a, emax=b, window_type="delta", mmax=mm, vectors=False))
+        return res_all
+
+    res_plain, t_plain = timed(plain)
+    g_plain, agree = [], []
+    for w, ((a, b), (lp, _, rp)) in enumerate(zip(wins, res_plain)):
+        okp = (lp >= a) & (lp <= b) & (rp <= 1e-10 * norm)
+        g_plain.append(int(okp.sum()))
+        sel = win == w
+        okq = (lam[sel] >= a) & (lam[sel] <= b) & (res[sel] <= 1e-10 * norm)
+        x, y = np.sort(lp[okp]), np.sort(lam[sel][okq])
+        agree.append(float(np.abs(x - y).max() / norm) if x.size == y.size and x.size else None)
+    out["plain_fp64"] = {"seconds": t_plain, "pairs": int(sum(g_plain)), "per_window": g_plain,
+                         "eigenpairs_per_s": sum(g_plain) / t_plain}
+    out["pipeline_over_plain"] = out["pipeline"]["eigenpairs_per_s"] / out["plain_fp64"]["eigenpairs_per_s"]
+    out["max_dlambda_over_norm_per_window"] = agree
+    print(json.dumps(out), flush=True)
+
+
 def run_profile_filter(args):
     """Only the block Clenshaw filter of the workload on device blocks
     (sma_apply_poly_block_dev), `calls` times: the small case for ncu captures of the
@@ -615,7 +731,9 @@ def main():
     ap.add_argument("--arm-steps", type=int, default=2,
                     help="timed solves of the plain and tuned arms (each after one warm-up)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c3", choices=["c2", "c3"])
+    ap.add_argument("--workload", default="c3", choices=["c2", "c3", "c4", "c5"],
+                    help="c4 / c5: one solve per arm of the batched pipeline and the plain path")
+    ap.add_argument("--no-plain", action="store_true", help="c4 / c5: pipeline arm only")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "fp32", "mixed"],
                     help="filter arithmetic of the pipeline arm (and of --profile-filter)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
@@ -639,6 +757,9 @@ def main():
         return
     if args.profile_slice:
         run_profile_slice(args)
+        return
+    if args.workload in ("c4", "c5"):
+        run_multi(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

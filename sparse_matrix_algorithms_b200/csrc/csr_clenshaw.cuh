@@ -38,13 +38,8 @@ __device__ __forceinline__ void epilogue(T *__restrict__ out, const T (&acc)[V],
                                          T alpha, T beta) {
   T r[V];
 #pragma unroll
-  for (int v = 0; v < V; ++v) {
-    T x = alpha * acc[v];
-    if constexpr (HQ) x = ck[v] * q[v] + x;
-    if constexpr (HS) x = x + beta * s[v];
-    if constexpr (HB) x = x - t[v];
-    r[v] = x;
-  }
+  for (int v = 0; v < V; ++v)
+    r[v] = clenshaw_combine<HQ, HS, HB>(acc[v], q[v], s[v], t[v], ck[v], alpha, beta);
   stv<T, V>(out, r);
 }
 

@@ -193,13 +193,8 @@ stencil_step_kernel(Rows rows, int64_t n, int b, const T *__restrict__ Q, int64_
       for (int v = 0; v < V; ++v) acc[v] = T(0);
       rows.template product<V>(prep, B1, ldb, c0, acc);
 #pragma unroll
-      for (int v = 0; v < V; ++v) {
-        T x = alpha * acc[v];
-        if constexpr (HAS_Q) x = ck * q[v] + x;
-        if constexpr (HAS_SELF) x = x + beta * s[v];
-        if constexpr (HAS_B2) x = x - t[v];
-        r[v] = x;
-      }
+      for (int v = 0; v < V; ++v)
+        r[v] = clenshaw_combine<HAS_Q, HAS_SELF, HAS_B2>(acc[v], q[v], s[v], t[v], ck, alpha, beta);
       stv<T, V>(out + row * ldo + c0, r);
     }
   }
@@ -273,7 +268,7 @@ __global__ void scale_block_kernel(int64_t n, int64_t b, const T *__restrict__ Q
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = t / b, j = t % b;
-    out[i * ldo + j] = ck * Q[i * ldq + j];
+    out[i * ldo + j] = mul_rn(ck, Q[i * ldq + j]);
   }
 }
 
@@ -287,9 +282,9 @@ __global__ void clenshaw_axpy_kernel(int64_t n, int64_t b, const T *__restrict__
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = t / b, j = t % b;
-    T x = ck * Q[i * ldq + j] + alpha * AX[i * ldax + j] + beta * B1[i * ldb + j];
-    if (B2) x = x - B2[i * ldb + j];
-    out[i * ldo + j] = x;
+    const T q = Q[i * ldq + j], a = AX[i * ldax + j], s = B1[i * ldb + j];
+    out[i * ldo + j] = B2 ? clenshaw_combine<true, true, true>(a, q, s, B2[i * ldb + j], ck, alpha, beta)
+                          : clenshaw_combine<true, true, false>(a, q, s, T(0), ck, alpha, beta);
   }
 }
 

@@ -160,7 +160,7 @@ clenshaw_persistent_kernel(const int *__restrict__ rowptr, const int *__restrict
         T q[V], r[V];
         ldv<T, V>(Q + (int64_t)row * ldq + c0, q);
 #pragma unroll
-        for (int v = 0; v < V; ++v) r[v] = ck * q[v];
+        for (int v = 0; v < V; ++v) r[v] = mul_rn(ck, q[v]);
         stv<T, V>(B1 + (int64_t)row * ldb + c0, r);
       }
     }
@@ -188,13 +188,9 @@ clenshaw_persistent_kernel(const int *__restrict__ rowptr, const int *__restrict
         row_product<T, V, U>(colind, val, start, end, B1 + c0, ldb, acc);
         T r[V];
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          T x = a * acc[v];
-          x = ck * q[v] + x;
-          x = x + bt * s[v];
-          if (has_b2) x = x - t[v];
-          r[v] = x;
-        }
+        for (int v = 0; v < V; ++v)
+          r[v] = has_b2 ? clenshaw_combine<true, true, true>(acc[v], q[v], s[v], t[v], ck, a, bt)
+                        : clenshaw_combine<true, true, false>(acc[v], q[v], s[v], T(0), ck, a, bt);
         stv<T, V>(out + (int64_t)row * ldo + c0, r);
       }
     }

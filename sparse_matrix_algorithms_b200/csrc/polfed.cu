@@ -208,11 +208,18 @@ class PolfedWindow {
     // converges at the ratio p(first outside)/p(window edge), which is close to 1.
     DevBuf<double> guard;
     int64_t ng = 0;
+    double guard_lo = o.emin, guard_hi = o.emax;  // the span of the guards' Ritz values
+    const PolishConfig pc = polish_config();
     if (o.precision == SMA_PREC_MIXED) {
       std::vector<int64_t> outw;
-      const int64_t want = std::max<int64_t>(1, ((int64_t)idx_keep.size() + 1) / 2);
+      const int64_t want =
+          std::max<int64_t>(1, (int64_t)std::ceil(pc.guard_fraction * (double)idx_keep.size()));
       for (int64_t jj = 0; jj < m && (int64_t)outw.size() < want; ++jj)
-        if (!(o.emin <= rs.lam[jj] && rs.lam[jj] <= o.emax)) outw.push_back(jj);
+        if (!(o.emin <= rs.lam[jj] && rs.lam[jj] <= o.emax)) {
+          outw.push_back(jj);
+          guard_lo = std::min(guard_lo, rs.lam[jj]);
+          guard_hi = std::max(guard_hi, rs.lam[jj]);
+        }
       ng = (int64_t)outw.size();
       if (ng > 0) {
         guard.alloc(n * ng, st_);
@@ -286,9 +293,37 @@ class PolfedWindow {
         std::sort(r.begin(), r.end());
         return r[std::min<size_t>(nev, r.size()) - 1] < o.tol;
       };
+      // the polish polynomial: the basis filter, or an undamped step over the window
+      // widened to the guards' span (sharper edges: the guards take the transition)
+      std::vector<double> pcoef = coeffs;
+      const int64_t Kp = std::max<int64_t>(
+          1, (int64_t)std::llround(pc.degree_scale * (double)(coeffs.size() - 1)));
+      if (pc.step_filter)
+        pcoef = build_coeffs(Kp, o.smin, o.smax, 0.5 * (guard_lo + guard_hi), guard_lo, guard_hi,
+                             SMA_WINDOW_STEP, false);
+      else if (Kp != (int64_t)coeffs.size() - 1)
+        pcoef = build_coeffs(Kp, o.smin, o.smax, o.sigma, o.emin, o.emax, o.window_type,
+                             o.jackson != 0);
+      auto needs = [&](double lam, double res) {  // guards and unconverged in-window pairs
+        return !(o.emin <= lam && lam <= o.emax) || res >= 0.5 * o.tol;
+      };
+      PolishTrace trace;
+      if (pc.verbose)
+        trace = [&](int64_t pass, const std::vector<double> &lam, const std::vector<double> &res) {
+          int64_t in = 0, ok = 0;
+          double mx = 0.0;
+          for (size_t i = 0; i < lam.size(); ++i)
+            if (o.emin <= lam[i] && lam[i] <= o.emax) {
+              ++in;
+              ok += res[i] < o.tol;
+              mx = std::max(mx, res[i]);
+            }
+          fprintf(stderr, "polish pass %lld: k=%lld in-window=%lld converged=%lld max-res=%.3e\n",
+                  (long long)pass, (long long)k, (long long)in, (long long)ok, mx);
+        };
       clk.mark(PH_FILTER);
-      const PolishOut po = polish_mixed(op_, coeffs, o.smin, o.smax, Xpol_.p, k, done, 3, polish,
-                                        &stats.qr_fallbacks);
+      const PolishOut po = polish_mixed(op_, pcoef, o.smin, o.smax, Xpol_.p, k, done, needs,
+                                        pc.max_passes, polish, &stats.qr_fallbacks, trace);
       clk.close();
       stats.polish_iterations += po.passes;
       // keep the in-window pairs, as the refinement does

@@ -26,38 +26,48 @@
 // only post-processing is Rayleigh-Ritz (refine_original_rr, polfed.jl:837-880); this
 // filtered pass is what an FP32 basis needs on top of it to reach its tolerance.
 #include <cmath>
+#include <cstdlib>
+#include <string>
 
 #include "solver_common.h"
+#include "vec.cuh"
 
 namespace sma {
 namespace {
 
-// R32[i, j] = (AX[i, j] - theta[j] X[i, j]) * inv_s[j] for j < k, 0 for k <= j < kpad.
-__global__ void residual_f32_kernel(int64_t n, int64_t k, int64_t kpad, const double *__restrict__ X,
-                                    int64_t ldx, const double *__restrict__ AX, int64_t ldax,
+// Residual block of the filtered columns: R[i, a] = (AX[i, j] - theta[j] X[i, j]) inv_s[j]
+// for j = act[a], a < ka; zero for ka <= a < kapad (padding to full vector width).
+__global__ void residual_f32_kernel(int64_t n, int64_t ka, int64_t kapad, const int *__restrict__ act,
+                                    const double *__restrict__ X, int64_t ldx,
+                                    const double *__restrict__ AX, int64_t ldax,
                                     const double *__restrict__ theta,
-                                    const double *__restrict__ inv_s, float *__restrict__ R,
-                                    int64_t ldr) {
-  const int64_t total = n * kpad;
+                                    const double *__restrict__ inv_s, float *__restrict__ R) {
+  const int64_t total = n * kapad;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = t / kpad, j = t % kpad;
+    const int64_t i = t / kapad, a = t % kapad;
     float v = 0.f;
-    if (j < k) v = (float)((AX[i * ldax + j] - theta[j] * X[i * ldx + j]) * inv_s[j]);
-    R[i * ldr + j] = v;
+    if (a < ka) {
+      const int j = act[a];
+      v = (float)((AX[i * ldax + j] - theta[j] * X[i * ldx + j]) * inv_s[j]);
+    }
+    R[i * kapad + a] = v;
   }
 }
 
-// Y[i, j] = pt[j] X[i, j] + sd[j] Z[i, j] (FP64 result from the FP32 correction block).
+// Y[i, j] = pt[j] X[i, j] + sd[j] Z[i, slot[j]] for filtered columns (slot[j] >= 0), and
+// Y[i, j] = X[i, j] for the others (FP64 result from the FP32 correction block).
 __global__ void combine_kernel(int64_t n, int64_t k, const double *__restrict__ X, int64_t ldx,
-                               const float *__restrict__ Z, int64_t ldz,
+                               const float *__restrict__ Z, int64_t ldz, const int *__restrict__ slot,
                                const double *__restrict__ pt, const double *__restrict__ sd,
                                double *__restrict__ Y, int64_t ldy) {
   const int64_t total = n * k;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = t / k, j = t % k;
-    Y[i * ldy + j] = pt[j] * X[i * ldx + j] + sd[j] * (double)Z[i * ldz + j];
+    const int a = slot[j];
+    const double x = X[i * ldx + j];
+    Y[i * ldy + j] = a >= 0 ? pt[j] * x + sd[j] * (double)Z[i * ldz + a] : x;
   }
 }
 
@@ -73,7 +83,7 @@ __global__ void percol_axpy_kernel(int64_t n, int64_t b, const T *__restrict__ Q
        t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = t / b, j = t % b;
     const int64_t e = i * ld + j;
-    out[e] = crow[j] * Q[e] + alpha * AX[e] + beta * B1[e] - B2[e];
+    out[e] = clenshaw_combine<true, true, true>(AX[e], Q[e], B1[e], B2[e], crow[j], alpha, beta);
   }
 }
 
@@ -154,9 +164,20 @@ void divided_difference(const std::vector<double> &c, double t, double *e, doubl
 
 using detail::dev_to_host;
 
+PolishConfig polish_config() {
+  PolishConfig c;
+  if (const char *f = std::getenv("SMA_POLISH_FILTER")) c.step_filter = std::string(f) == "step";
+  if (const char *g = std::getenv("SMA_POLISH_GUARDS")) c.guard_fraction = std::max(0.0, std::atof(g));
+  if (const char *d = std::getenv("SMA_POLISH_DEGREE")) c.degree_scale = std::max(0.05, std::atof(d));
+  if (const char *p = std::getenv("SMA_POLISH_PASSES")) c.max_passes = std::max(0, std::atoi(p));
+  if (const char *v = std::getenv("SMA_POLISH_VERBOSE")) c.verbose = std::string(v) == "1";
+  return c;
+}
+
 PolishOut polish_mixed(const sma_op *op, const std::vector<double> &coeffs, double smin,
                        double smax, double *X, int64_t k, const PolishDone &done,
-                       int64_t max_passes, FilterCount &fc, int64_t *qr_fallbacks) {
+                       const PolishNeeds &needs, int64_t max_passes, FilterCount &fc,
+                       int64_t *qr_fallbacks, const PolishTrace &trace) {
   PolishOut out;
   sma_ctx *ctx = op->ctx;
   cudaStream_t st = ctx->stream;
@@ -171,7 +192,7 @@ PolishOut polish_mixed(const sma_op *op, const std::vector<double> &coeffs, doub
   DevBuf<float> R32(n * kpad, st), Z32(n * kpad, st), B1(n * kpad, st), B2(n * kpad, st),
       TMP(n * kpad, st), AX32, coef32(K * kpad, st);
   if (op->kind != OP_CSR) AX32.alloc(n * kpad, st);
-  DevBuf<int> colseg(kpad, st);
+  DevBuf<int> colseg(kpad, st), act_d(kpad, st), slot_d(k, st);
   {
     std::vector<int> idn(kpad);
     for (int64_t j = 0; j < kpad; ++j) idn[j] = (int)j;
@@ -195,34 +216,51 @@ PolishOut polish_mixed(const sma_op *op, const std::vector<double> &coeffs, doub
   // consistent start: Rayleigh-Ritz on the candidates themselves
   SMA_CUDA(cudaMemcpyAsync(Y.p, X, n * k * sizeof(double), cudaMemcpyDeviceToDevice, st));
   rayleigh_ritz(Y.p);
-  std::vector<double> ch(K * kpad), inv_s(k), pt(k), sd(k);
-  std::vector<float> cf(K * kpad, 0.f);
-  std::vector<double> e(K);
+  if (trace) trace(0, out.lam, out.res);
+  std::vector<double> inv_s(k), pt(k), sd(k), e(K);
+  std::vector<float> cf;
+  std::vector<int> act, slot(k);
   for (int64_t pass = 0; pass < max_passes && !done(out.lam, out.res); ++pass) {
+    // the columns to filter: all of them in the first pass, then those the caller still needs
+    act.clear();
     for (int64_t j = 0; j < k; ++j) {
+      const bool f = pass == 0 || needs(out.lam[j], out.res[j]);
+      slot[j] = f ? (int)act.size() : -1;
+      if (f) act.push_back((int)j);
+    }
+    const int64_t ka = (int64_t)act.size(), kapad = (ka + 7) / 8 * 8;
+    if (ka == 0) break;
+    cf.assign(K * kapad, 0.f);
+    for (int64_t a = 0; a < ka; ++a) {
+      const int64_t j = act[a];
       const double s = out.res[j];
       inv_s[j] = s > 0.0 ? 1.0 / s : 0.0;
       sd[j] = s / d;
       divided_difference(coeffs, (out.lam[j] - c) / d, e.data(), &pt[j]);
-      for (int64_t m = 0; m < K; ++m) cf[m * kpad + j] = (float)e[m];
+      for (int64_t m = 0; m < K; ++m) cf[m * kapad + a] = (float)e[m];
     }
     SMA_CUDA(cudaMemcpyAsync(theta_d.p, out.lam.data(), k * sizeof(double), cudaMemcpyHostToDevice, st));
     SMA_CUDA(cudaMemcpyAsync(inv_s_d.p, inv_s.data(), k * sizeof(double), cudaMemcpyHostToDevice, st));
     SMA_CUDA(cudaMemcpyAsync(pt_d.p, pt.data(), k * sizeof(double), cudaMemcpyHostToDevice, st));
     SMA_CUDA(cudaMemcpyAsync(sd_d.p, sd.data(), k * sizeof(double), cudaMemcpyHostToDevice, st));
+    SMA_CUDA(cudaMemcpyAsync(act_d.p, act.data(), ka * sizeof(int), cudaMemcpyHostToDevice, st));
+    SMA_CUDA(cudaMemcpyAsync(slot_d.p, slot.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
     SMA_CUDA(cudaMemcpyAsync(coef32.p, cf.data(), cf.size() * sizeof(float), cudaMemcpyHostToDevice, st));
-    residual_f32_kernel<<<grid_of(n * kpad), 256, 0, st>>>(n, k, kpad, X, k, AX.p, k, theta_d.p,
-                                                          inv_s_d.p, R32.p, kpad);
+    residual_f32_kernel<<<grid_of(n * kapad), 256, 0, st>>>(n, ka, kapad, act_d.p, X, k, AX.p, k,
+                                                           theta_d.p, inv_s_d.p, R32.p);
     SMA_CHECK_LAUNCH();
     const FilterCount f = percol_filter<float>(op, st, coef32.p, K - 1, smin, smax, R32.p, Z32.p,
-                                               kpad, colseg.p, B1.p, B2.p, TMP.p, AX32.p);
+                                               kapad, colseg.p, B1.p, B2.p, TMP.p, AX32.p);
     fc.steps += f.steps;
     fc.bytes += f.bytes;
-    combine_kernel<<<grid_of(n * k), 256, 0, st>>>(n, k, X, k, Z32.p, kpad, pt_d.p, sd_d.p, Y.p, k);
+    combine_kernel<<<grid_of(n * k), 256, 0, st>>>(n, k, X, k, Z32.p, kapad, slot_d.p, pt_d.p,
+                                                   sd_d.p, Y.p, k);
     SMA_CHECK_LAUNCH();
     rayleigh_ritz(Y.p);
     SMA_CUDA(cudaStreamSynchronize(st));  // the host tables above are rewritten next pass
     out.passes += 1;
+    out.columns += ka;
+    if (trace) trace(out.passes, out.lam, out.res);
   }
   return out;
 }

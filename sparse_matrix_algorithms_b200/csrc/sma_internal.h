@@ -378,15 +378,36 @@ void divided_difference(const std::vector<double> &c, double t, double *e, doubl
 struct PolishOut {
   std::vector<double> lam, res;  // Ritz values (ascending) and residual norms of X
   int64_t passes = 0;
+  int64_t columns = 0;  // columns filtered, summed over the passes
 };
-// done(lam, res) ends the passes early.
+// done(lam, res) ends the passes early; trace(pass, lam, res) sees every pass (pass 0: the
+// Rayleigh-Ritz of the candidates before any filtering); needs(lam, res): whether a column
+// is filtered again after the first pass (converged in-window columns pass through to the
+// Rayleigh-Ritz unchanged).
 using PolishDone = std::function<bool(const std::vector<double> &, const std::vector<double> &)>;
+using PolishTrace =
+    std::function<void(int64_t, const std::vector<double> &, const std::vector<double> &)>;
+using PolishNeeds = std::function<bool(double, double)>;
+// Polish settings, from the environment: SMA_POLISH_FILTER=step (an undamped step window
+// over the guards' span) or same (the basis filter, default); SMA_POLISH_GUARDS (guards as a
+// fraction of the in-window candidates, default 0.5); SMA_POLISH_DEGREE (degree scale of the
+// polish polynomial, default 1); SMA_POLISH_PASSES (default 3); SMA_POLISH_VERBOSE=1.
+struct PolishConfig {
+  bool step_filter = false;
+  double guard_fraction = 0.5;
+  double degree_scale = 1.0;
+  int64_t max_passes = 3;
+  bool verbose = false;
+};
+PolishConfig polish_config();
 // Rayleigh-Ritz with A on the k columns of X (n x k, ld k, FP64, in place), then up to
 // max_passes filtered subspace iterations with p = sum coeffs[m] T_m(A_hat), each applying
-// p as p(theta) x + q_theta(A_hat) r / d with q in FP32; X ends as the last Ritz vectors.
+// p as p(theta) x + q_theta(A_hat) r / d with q in FP32 (the first pass on every column,
+// later passes on the columns needs() selects); X ends as the last Ritz vectors.
 PolishOut polish_mixed(const sma_op *op, const std::vector<double> &coeffs, double smin,
                        double smax, double *X, int64_t k, const PolishDone &done,
-                       int64_t max_passes, FilterCount &fc, int64_t *qr_fallbacks);
+                       const PolishNeeds &needs, int64_t max_passes, FilterCount &fc,
+                       int64_t *qr_fallbacks, const PolishTrace &trace = PolishTrace());
 
 // ------------------------------------------------------------------ result
 }  // namespace sma

@@ -57,3 +57,31 @@ __device__ __forceinline__ void stv(T *__restrict__ p, const T (&f)[V]) {
 }
 
 }  // namespace sma
+
+namespace sma {
+
+// Round-to-nearest products and sums that the compiler never contracts into FMAs.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+
+// One element of a Clenshaw step's epilogue, ck*q + alpha*acc + beta*s - t, evaluated left
+// to right as the reference's broadcast TMP .= c_k .* Q .+ alpha .* AX .+ beta .* B1 .- B2
+// (chebyshev_subspace_iteration.jl:576-580) with every product and sum rounded on its own.
+// Left to the compiler, ck*q + alpha*acc may be fused either way round into an FMA, and
+// different kernels would then round differently; with this form every kernel that takes a
+// step -- CSR, segmented, stencil, persistent, matrix-free axpy -- writes the same bits.
+// HQ, HS, HB: whether the q, s and t terms are present.
+template <bool HQ, bool HS, bool HB, typename T>
+__device__ __forceinline__ T clenshaw_combine(T acc, T q, T s, T t, T ck, T alpha, T beta) {
+  T x = mul_rn(alpha, acc);
+  if constexpr (HQ) x = add_rn(mul_rn(ck, q), x);
+  if constexpr (HS) x = add_rn(x, mul_rn(beta, s));
+  if constexpr (HB) x = sub_rn(x, t);
+  return x;
+}
+
+}  // namespace sma

@@ -21,7 +21,7 @@ module SparseMatrixAlgorithmsB200
 using SparseArrays
 using LinearAlgebra
 
-export chebyshev_poly_real_symm_sparse, polfed, MatrixFreeRealSymOp, DeviceCSR, Lap1dDevice,
+export chebyshev_poly_real_symm_sparse, polfed, polfed_windows, MatrixFreeRealSymOp, DeviceCSR, Lap1dDevice,
        AndersonDevice, XXZDevice, DeviceMatblock, gershgorin_bounds, lanczos_bounds,
        jackson_kernel, cheb_delta_coeffs, cheb_window_coeffs, cheb_smooth_window_coeffs,
        kpm_moments, kpm_count, slice_spectrum
@@ -355,6 +355,41 @@ function slice_spectrum(op::DeviceCSR, windows::Vector{Tuple{Float64,Float64}}, 
     check(ccall((:sma_slice_solve, libsma), Cint,
                 (Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Ptr{Int64}, Ptr{Int64}, Ref{SliceOpts}, Ref{Ptr{Cvoid}}),
                 op.handle, length(windows), emin, emax, Int64.(degrees), Int64.(m0s), o, h))
+    k = Ref{Int64}(0); nn = Ref{Int64}(0)
+    check(ccall((:sma_result_count, libsma), Cint, (Ptr{Cvoid}, Ref{Int64}, Ref{Int64}), h[], k, nn))
+    win = Vector{Int64}(undef, k[])
+    k[] > 0 && check(ccall((:sma_result_windows, libsma), Cint, (Ptr{Cvoid}, Ptr{Int64}), h[], win))
+    λ, X, res = take_result(h[])
+    return λ, X, res, win .+ 1
+end
+
+"""
+    polfed_windows(op::DeviceCSR, windows, nevs, degrees, mmaxs; kwargs...) -> (λ, X, res, win)
+
+Batched POLFED (an extension; `polfed` solves one window): window w is a POLFED solve with
+its own nev, degree and mmax, its filter centred on the window and start seed `seed + w - 1`;
+every block step filters all windows' blocks in ONE segmented recurrence.  Keyword
+arguments as `polfed` (s, smin, smax, tol, window_type, jackson, precision, ...).  `win[j]`
+is the (1-based) window of pair j; each window's pairs follow polfed's return order.
+"""
+function polfed_windows(op::DeviceCSR, windows::Vector{Tuple{Float64,Float64}}, nevs::Vector{Int},
+        degrees::Vector{Int}, mmaxs::Vector{Int}; s::Int=8, smin::Float64, smax::Float64,
+        tol::Float64=1e-10, overextract::Int=2, refine::Bool=true, window_type::Symbol=:step,
+        jackson::Bool=true, rtol::Float64=1e-12, reorth_passes::Int=1, extra_keep::Int=8,
+        seed::Int=1, show_progress::Bool=false, precision::Symbol=:fp64)
+    o = PolfedOpts()
+    ccall((:sma_polfed_opts_default, libsma), Cvoid, (Ref{PolfedOpts},), o)
+    o.s = s; o.smin = smin; o.smax = smax; o.has_bounds = 1; o.tol = tol
+    o.overextract = overextract; o.refine = refine; o.window_type = window_code(window_type)
+    o.jackson = jackson; o.rtol = rtol; o.reorth_passes = reorth_passes
+    o.extra_keep = extra_keep; o.seed = seed; o.show_progress = show_progress
+    o.precision = precision_code(precision)
+    emin = first.(windows); emax = last.(windows)
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:sma_polfed_batch_solve, libsma), Cint,
+                (Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Ptr{Int64}, Ptr{Int64}, Ptr{Int64},
+                 Ref{PolfedOpts}, Ref{Ptr{Cvoid}}),
+                op.handle, length(windows), emin, emax, Int64.(nevs), Int64.(degrees), Int64.(mmaxs), o, h))
     k = Ref{Int64}(0); nn = Ref{Int64}(0)
     check(ccall((:sma_result_count, libsma), Cint, (Ptr{Cvoid}, Ref{Int64}, Ref{Int64}), h[], k, nn))
     win = Vector{Int64}(undef, k[])

@@ -336,8 +336,8 @@ def windows_by_count(mu, n: int, smin: float, smax: float, center: float,
 # configuration of this library's POLFED sweeps).
 POLFED_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "planner_data",
                               "polfed_planner_weights.npz")
-POLFED_GRID_K = (0.4, 0.55, 0.75, 1.0)
-POLFED_GRID_M = (1.0, 1.5, 2.0)
+POLFED_GRID_K = (0.25, 0.33, 0.45, 0.6, 0.8, 1.0)
+POLFED_GRID_M = (1.0, 1.5, 2.0, 2.7)
 
 
 def polfed_plain_rule(count: float, smin: float, smax: float, emin: float, emax: float,
@@ -502,6 +502,54 @@ def solve_polfed_windows(A, windows, planner: Optional[WindowPlanner] = None, *,
                            good=[_polfed_good(lam[win == w], res[win == w], *windows[w], nrm)
                                  for w in ids]))
     return lam, X, res, win
+
+
+def polfed_training_rows_batched(A, windows, *, s: int = 32, smin: float, smax: float,
+                                 mu: np.ndarray, grid_k: Iterable[float] = POLFED_GRID_K,
+                                 grid_m: Iterable[float] = POLFED_GRID_M, seed: int = 1):
+    """Training rows from plain-solver POLFED runs (FP64, Jackson-damped delta filter) at a
+    grid of (degree, mmax) scales of the plain rule: every (window, scale) pair is one
+    window of ONE batched POLFED call (sma_polfed_batch_solve), so the matrix is read once
+    per step for all of them.  The target is the cheapest run (column-steps) that found as
+    many converged in-window pairs as the best run, and log(found / KPM count)."""
+    from .api import polfed_windows
+
+    op = _op_of(A)
+    nrm = max(abs(smin), abs(smax))
+    grid = [(sk, sm) for sk in grid_k for sm in grid_m]
+    wins, nevs, degs, mms, meta = [], [], [], [], []
+    for wi, (a, b) in enumerate(windows):
+        N = kpm_count(mu, op.n, smin, smax, a, b)
+        K0, m0 = polfed_plain_rule(N, smin, smax, a, b, s)
+        for sk, sm in grid:
+            wins.append((a, b))
+            nevs.append(polfed_nev(N))
+            degs.append(max(1, int(round(K0 * sk))))
+            mms.append(max(2, int(math.ceil(m0 * sm))))
+            meta.append((wi, sk, sm, N))
+    lam, _, res, win = polfed_windows(op, wins, nevs, degs, mms, s=s, smin=smin, smax=smax,
+                                      window_type="delta", seed=seed, vectors=False)
+    F, T, W = [], [], []
+    for wi, (a, b) in enumerate(windows):
+        runs = []
+        for j, (wj, sk, sm, N) in enumerate(meta):
+            if wj != wi:
+                continue
+            sel = win == j
+            runs.append((sk, sm, polfed_cost(degs[j], mms[j], s),
+                         _polfed_good(lam[sel], res[sel], a, b, nrm), N))
+        ref = max(r[3] for r in runs)
+        f = window_features(mu, smin, smax, a, b)
+        ok = [r for r in runs if r[3] == ref and ref > 0]
+        if not ok:
+            F.append(f); T.append(np.zeros(OUT_DIM, np.float32)); W.append(np.zeros(OUT_DIM, np.float32))
+            continue
+        best = min(ok, key=lambda r: r[2])
+        F.append(f)
+        T.append(np.array([math.log(best[0]), math.log(best[1]), math.log(ref / max(best[4], 1.0))],
+                          np.float32))
+        W.append(np.ones(OUT_DIM, np.float32))
+    return np.stack(F), np.stack(T), np.stack(W)
 
 
 def polfed_training_rows(A, windows, *, s: int = 8, smin=None, smax=None, mu=None,

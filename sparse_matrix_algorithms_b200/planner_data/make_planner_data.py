@@ -8,9 +8,13 @@
 in [2, 20]) and the XXZ chain (L in 12..16, h uniform in [0.5, 8]) -- places windows of
 12..64 KPM-estimated eigenvalues in the bulk of each spectrum, and solves every window at
 the grid of (degree, width) scales of the plain rule in one batched slicing call per
-matrix (``planner.training_rows``).  ``train`` fits the network on the GPU with the
-library's own kernels.  Needs a GPU.  Matrices are smaller than the sizes the planner is
-meant to serve; the features (KPM moments and mapped window bounds) do not depend on n.
+matrix (``planner.training_rows``).  ``gen-polfed`` does the same for POLFED on matrices
+of the target distribution -- Anderson L in 16..48 (W in [2, 20]), XXZ L in 14..18 (h in
+[0.5, 8]) -- with windows of 40..400 eigenvalues, Lanczos bounds as the pipeline uses them,
+and every window's scale grid run as ONE batched POLFED call
+(``planner.polfed_training_rows_batched``).  ``train`` fits the network on the GPU with
+the library's own kernels.  Needs a GPU.  The features (KPM moments and mapped window
+bounds) do not depend on n.
 """
 import argparse
 import os
@@ -117,61 +121,90 @@ def evaluate(weights=P.WEIGHTS, problems=HELD_OUT, counts=(20, 45, 30), verbose=
 
 
 def sample_polfed_matrix(rng):
-    """Smaller matrices for the POLFED sweep: every window is solved 12 times."""
+    """The POLFED planner's training distribution: 3D Anderson, L in 16..48, W uniform in
+    [2, 20]; XXZ chain, L in 14..18, h uniform in [0.5, 8]."""
     if rng.uniform() < 0.6:
-        L = int(rng.choice([10, 12, 14]))
+        L = int(rng.choice([16, 20, 24, 28, 32, 40, 48]))
         W = float(rng.uniform(2.0, 20.0))
         seed = int(rng.integers(1 << 30))
         return f"anderson L={L} W={W:.3f} seed={seed}", M.anderson3d(L, W, seed)
-    L = int(rng.choice([12, 14]))
+    L = int(rng.choice([14, 16, 18]))
     h = float(rng.uniform(0.5, 8.0))
     seed = int(rng.integers(1 << 30))
     return f"xxz L={L} h={h:.3f} seed={seed}", M.xxz_sz0(L, h, seed)
 
 
+def sample_polfed_windows(rng, mu, n, smin, smax, k, lo_count, hi_count):
+    lo = P.energy_at_count(mu, n, smin, smax, smin, 0.2 * n)
+    hi = P.energy_at_count(mu, n, smin, smax, smin, 0.8 * n)
+    out = []
+    for _ in range(k):
+        c = float(rng.uniform(lo, hi))
+        N = float(np.exp(rng.uniform(np.log(lo_count), np.log(min(hi_count, 0.02 * n)))))
+        out.append(P.windows_by_count(mu, n, smin, smax, c, [N])[0])
+    return out
+
+
 def gen_polfed(args):
+    """Lanczos bounds (100 steps) and KPM moments on them, as the pipeline computes them;
+    every window's scale grid of the plain rule solved in one batched POLFED call."""
     rng = np.random.default_rng(args.seed)
     F, T, W, names = [], [], [], []
     t0 = time.time()
     for i in range(args.matrices):
         name, A = sample_polfed_matrix(rng)
         op = S.SparseOperator(A)
-        smin, smax = op.gershgorin_bounds()
+        smin, smax = S.lanczos_bounds(op, steps=100)
         mu = S.kpm_moments(op, P.N_MOMENTS, 16, smin=smin, smax=smax)
-        wins = sample_windows(rng, mu, A.shape[0], smin, smax, args.windows)
-        f, t, w = P.polfed_training_rows(op, wins, smin=smin, smax=smax, mu=mu)
+        wins = sample_polfed_windows(rng, mu, A.shape[0], smin, smax, args.windows, args.min_count,
+                                     args.max_count)
+        rows = [P.polfed_training_rows_batched(op, [win], s=args.s, smin=smin, smax=smax, mu=mu)
+                for win in wins]  # one window (its whole scale grid) per batched call
+        f, t, w = (np.concatenate([r[i] for r in rows]) for i in range(3))
         F.append(f); T.append(t); W.append(w); names += [name] * len(wins)
         print(f"{i + 1}/{args.matrices} {name}: {int(w[:, 0].sum())}/{len(wins)} windows usable, "
-              f"{time.time() - t0:.1f} s", flush=True)
-    np.savez_compressed(args.out, X=np.concatenate(F), T=np.concatenate(T), W=np.concatenate(W),
-                        names=np.array(names))
+              f"targets {np.round(np.exp(t[:, :2]), 2).tolist()}, {time.time() - t0:.1f} s", flush=True)
+        op.close()
+        np.savez_compressed(args.out, X=np.concatenate(F), T=np.concatenate(T),
+                            W=np.concatenate(W), names=np.array(names))
 
 
-def evaluate_polfed(weights=P.POLFED_WEIGHTS, problems=HELD_OUT, counts=(30, 50), verbose=True):
+HELD_OUT_POLFED = [("anderson", 24, 12.0, 77), ("anderson", 32, 4.0, 78), ("xxz", 16, 3.0, 79),
+                   ("xxz", 18, 6.5, 80)]
+
+
+def evaluate_polfed(weights=P.POLFED_WEIGHTS, problems=HELD_OUT_POLFED, counts=(60, 150),
+                    verbose=True, s=32):
     """Column-steps of POLFED's plain rule and of the learned plan (fallback included) on
-    held-out matrices, and whether both found the same converged eigenvalues."""
+    held-out matrices of the training distribution -- both windows of a matrix in one
+    batched call per planner -- and whether both found the same converged eigenvalues."""
     net = P.WindowPlanner.load(weights)
     rows = []
     for kind, L, p, seed in problems:
         A = held_out_problem(kind, L, p, seed)
         op = S.SparseOperator(A)
-        smin, smax = op.gershgorin_bounds()
+        smin, smax = S.lanczos_bounds(op, steps=100)
         nrm = max(abs(smin), abs(smax))
         mu = S.kpm_moments(op, P.N_MOMENTS, 16, smin=smin, smax=smax)
         centre = P.energy_at_count(mu, A.shape[0], smin, smax, smin, 0.5 * A.shape[0])
-        for win in P.windows_by_count(mu, A.shape[0], smin, smax, centre, counts):
-            rp, rl = {}, {}
-            lp, _, resp = P.solve_polfed_window(op, win, None, smin=smin, smax=smax, mu=mu, report=rp)
-            ll, _, resl = P.solve_polfed_window(op, win, net, smin=smin, smax=smax, mu=mu, report=rl)
-            gp = np.sort(lp[(lp >= win[0]) & (lp <= win[1]) & (resp <= 1e-10 * nrm)])
-            gl = np.sort(ll[(ll >= win[0]) & (ll <= win[1]) & (resl <= 1e-10 * nrm)])
+        wins = P.windows_by_count(mu, A.shape[0], smin, smax, centre, counts)
+        rp, rl = {}, {}
+        lp, _, resp, wp = P.solve_polfed_windows(op, wins, None, s=s, smin=smin, smax=smax, mu=mu,
+                                                 report=rp, vectors=False)
+        ll, _, resl, wl = P.solve_polfed_windows(op, wins, net, s=s, smin=smin, smax=smax, mu=mu,
+                                                 report=rl, vectors=False)
+        for w, win in enumerate(wins):
+            sp, sl = wp == w, wl == w
+            gp = np.sort(lp[sp][(lp[sp] >= win[0]) & (lp[sp] <= win[1]) & (resp[sp] <= 1e-10 * nrm)])
+            gl = np.sort(ll[sl][(ll[sl] >= win[0]) & (ll[sl] <= win[1]) & (resl[sl] <= 1e-10 * nrm)])
             same = gp.size == gl.size and (gp.size == 0 or float(np.abs(gp - gl).max()) <= 1e-12 * nrm)
-            row = dict(problem=f"{kind} L={L} p={p} seed={seed}", window=win, plain=rp["cost"],
-                       learned=rl["cost"], redone=rl["redone"], same=same, found=int(gp.size),
-                       plain_plan=rp["plan"], learned_plan=rl["plan"])
+            row = dict(problem=f"{kind} L={L} p={p} seed={seed}", window=win, plain=rp["cost"][w],
+                       learned=rl["cost"][w], redone=w in rl["redone"], same=same, found=int(gp.size),
+                       plain_plan=rp["plan"][w], learned_plan=rl["plan"][w])
             rows.append(row)
             if verbose:
                 print(row, flush=True)
+        op.close()
     return rows
 
 
@@ -194,9 +227,12 @@ def main():
     e = sub.add_parser("eval")
     e.add_argument("--weights", default=P.WEIGHTS)
     gp = sub.add_parser("gen-polfed")
-    gp.add_argument("--matrices", type=int, default=20)
-    gp.add_argument("--windows", type=int, default=3)
-    gp.add_argument("--seed", type=int, default=4048)
+    gp.add_argument("--matrices", type=int, default=24)
+    gp.add_argument("--windows", type=int, default=2)
+    gp.add_argument("--s", type=int, default=32)
+    gp.add_argument("--min-count", type=float, default=40)
+    gp.add_argument("--max-count", type=float, default=400)
+    gp.add_argument("--seed", type=int, default=4049)
     gp.add_argument("--out", default=os.path.join(HERE, "polfed_planner_train.npz"))
     tp_ = sub.add_parser("train-polfed")
     tp_.add_argument("--data", default=os.path.join(HERE, "polfed_planner_train.npz"))
