@@ -60,6 +60,7 @@ void free_op(sma_op *op) {
   if (op->colind) cudaFree(op->colind);
   if (op->val64) cudaFree(op->val64);
   if (op->val32) cudaFree(op->val32);
+  if (op->bulk_err) cudaFree(op->bulk_err);
   free_stencil_arrays(op);
   delete op;
 }

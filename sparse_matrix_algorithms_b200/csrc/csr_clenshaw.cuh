@@ -232,6 +232,142 @@ async_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
   }
 }
 
+// BULK family: a CTA of kBulkThreads threads owns RC = kBulkThreads / G rows (G threads of V
+// elements each cover a row in ONE pass, b = G V) and first stages everything its step
+// reads into shared memory: its CSR pairs (plain coalesced loads), then with 1D bulk copies
+// (cp.async.bulk global -> this CTA's shared memory; no multicast, local memory only) the
+// rows of Q, B1 and B2 it updates and every neighbour row of B1 its pairs name, all
+// completing on one mbarrier.  Every row a CTA needs is in flight at once without holding
+// registers, and the arithmetic reads shared memory only, in the same order as the other
+// families (bit-identical results).  Whole rows move, so rows must be 16..512 bytes and all
+// leading dimensions multiples of 16 bytes.  The host sizes the shared memory for the
+// largest CTA of the operator.  The wait on the mbarrier is bounded by elapsed time
+// (%globaltimer, one second): a CTA that gives up sets *err, waits (bounded again) for its
+// copies, and returns without writing; the host then reports SMA_ERR_TIMEOUT.
+constexpr int kBulkThreads = 256;
+constexpr unsigned long long kBulkWaitNs = 1000000000ull;
+
+__device__ __forceinline__ unsigned long long bulk_clock_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void bulk_copy(void *smem_dst, const void *gsrc, unsigned bytes,
+                                          unsigned mbar) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+      ::"r"(d), "l"(gsrc), "r"(bytes), "r"(mbar) : "memory");
+}
+
+// Waits for phase 0 of the mbarrier; false when `limit_ns` of elapsed time passed first.
+__device__ __forceinline__ bool bulk_wait(unsigned mbar, unsigned long long limit_ns) {
+  const unsigned long long t0 = bulk_clock_ns();
+  for (unsigned long long spin = 0;; ++spin) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done) : "r"(mbar) : "memory");
+    if (done) return true;
+    if (bulk_clock_ns() - t0 > limit_ns || spin > (1ull << 34)) return false;
+  }
+}
+
+template <typename T, int V, int G, bool HQ, bool HS, bool HB>
+__global__ void __launch_bounds__(kBulkThreads)
+bulk_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
+            const T *__restrict__ val, int64_t n, int b, const T *__restrict__ Q, int64_t ldq,
+            const T *__restrict__ B1, const T *__restrict__ B2, int64_t ldb,
+            T *__restrict__ out, int64_t ldo, T ck, T alpha, T beta, int cap, int *err) {
+  constexpr int RC = kBulkThreads / G;
+  constexpr int NR = (HQ ? 1 : 0) + (HS ? 1 : 0) + (HB ? 1 : 0);
+  extern __shared__ __align__(16) unsigned char bulk_smem[];
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(bulk_smem);
+  T *rows = reinterpret_cast<T *>(bulk_smem + 16);  // NR x RC rows: Q, B1, B2 (those present)
+  T *nbr = rows + (size_t)NR * RC * b;               // cap neighbour rows
+  T *sval = nbr + (size_t)cap * b;
+  int *scol = reinterpret_cast<int *>(sval + cap);
+  const unsigned mbar = static_cast<unsigned>(__cvta_generic_to_shared(bar));
+  const unsigned rb = (unsigned)b * sizeof(T);
+  const int64_t row0 = (int64_t)blockIdx.x * RC;
+  const int nrows = (int)min((int64_t)RC, n - row0);
+  const int base = __ldg(rowptr + row0);
+  const int cnt = __ldg(rowptr + row0 + nrows) - base;
+  if (cnt > cap) {  // the host sized shared memory for the largest CTA: never taken
+    if (threadIdx.x == 0) atomicExch(err, 2);
+    return;
+  }
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  for (int i = threadIdx.x; i < cnt; i += kBulkThreads) {
+    scol[i] = __ldg(colind + base + i);
+    sval[i] = __ldg(val + base + i);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned bytes = ((unsigned)cnt + (unsigned)(NR * nrows)) * rb;
+    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n"
+                 ::"r"(mbar), "r"(bytes) : "memory");
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < cnt; i += kBulkThreads)
+    bulk_copy(nbr + (size_t)i * b, B1 + (int64_t)scol[i] * ldb, rb, mbar);
+  {
+    int slot = 0;
+    const T *src[3];
+    int64_t ld[3];
+    if constexpr (HQ) { src[slot] = Q; ld[slot] = ldq; ++slot; }
+    if constexpr (HS) { src[slot] = B1; ld[slot] = ldb; ++slot; }
+    if constexpr (HB) { src[slot] = B2; ld[slot] = ldb; ++slot; }
+    for (int e = threadIdx.x; e < NR * nrows; e += kBulkThreads) {
+      const int k = e / nrows, r = e % nrows;
+      bulk_copy(rows + ((size_t)k * RC + r) * b, src[k] + (row0 + r) * ld[k], rb, mbar);
+    }
+  }
+  if (!bulk_wait(mbar, kBulkWaitNs)) {
+    if (threadIdx.x == 0) atomicExch(err, 1);
+    bulk_wait(mbar, kBulkWaitNs);  // let the copies in flight land before the CTA exits
+    return;
+  }
+  const int r = threadIdx.x / G;
+  if (r >= nrows) return;
+  const int c0 = (threadIdx.x % G) * V;
+  const int64_t row = row0 + r;
+  const int start = __ldg(rowptr + row) - base, end = __ldg(rowptr + row + 1) - base;
+  T acc[V], q[V], sv[V], t[V], ckv[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    acc[v] = T(0);
+    ckv[v] = ck;
+  }
+  for (int e = start; e < end; ++e) {
+    const T a = sval[e];
+    const T *x = nbr + (size_t)e * b + c0;
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] = fma(a, x[v], acc[v]);
+  }
+  int slot = 0;
+  if constexpr (HQ) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) q[v] = rows[((size_t)slot * RC + r) * b + c0 + v];
+    ++slot;
+  }
+  if constexpr (HS) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) sv[v] = rows[((size_t)slot * RC + r) * b + c0 + v];
+    ++slot;
+  }
+  if constexpr (HB) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) t[v] = rows[((size_t)slot * RC + r) * b + c0 + v];
+  }
+  epilogue<T, V, HQ, HS, HB>(out + row * ldo + c0, acc, q, sv, t, ckv, alpha, beta);
+}
+
 // ------------------------------------------------------------------ configurations
 // Encoded as fam | V << 4 | G << 8 | U << 16 (for the ASYNC family U is NB).
 inline int enc(int fam, int V, int G, int U) { return fam | (V << 4) | (G << 8) | (U << 16); }
@@ -306,9 +442,81 @@ void launch_async(const Args<T> &a) {
   SMA_CHECK_LAUNCH();
 }
 
+// The most CSR entries held by any CTA of RC consecutive rows (cached per RC).
+inline int bulk_max_pairs(const sma_op *op, int RC) {
+  sma_op *o = const_cast<sma_op *>(op);
+  const auto it = o->bulk_pairs.find(RC);
+  if (it != o->bulk_pairs.end()) return it->second;
+  if (o->host_rowptr.empty()) {
+    o->host_rowptr.resize(op->n + 1);
+    SMA_CUDA(cudaMemcpy(o->host_rowptr.data(), op->rowptr, (op->n + 1) * sizeof(int),
+                        cudaMemcpyDeviceToHost));
+  }
+  int mx = 0;
+  for (int64_t r = 0; r < op->n; r += RC) {
+    const int64_t e = std::min<int64_t>(op->n, r + RC);
+    mx = std::max(mx, o->host_rowptr[e] - o->host_rowptr[r]);
+  }
+  o->bulk_pairs[RC] = mx;
+  return mx;
+}
+
+inline size_t bulk_smem_bytes(int RC, int nr, int b, int cap, size_t elem) {
+  return 16 + (size_t)nr * RC * b * elem + (size_t)cap * (b * elem + elem + sizeof(int));
+}
+
+template <typename T, int V, int G, bool HQ, bool HS, bool HB>
+void launch_bulk(const Args<T> &a) {
+  if (a.cseg) throw Error(SMA_ERR_INTERNAL, "the bulk family has no segmented variant");
+  const sma_op *op = a.op;
+  if (a.b != (int64_t)G * V) throw Error(SMA_ERR_INTERNAL, "bulk family: b != G V");
+  const T *val;
+  if constexpr (sizeof(T) == 8) val = (const T *)op->val64;
+  else val = (const T *)op->val32;
+  constexpr int RC = kBulkThreads / G;
+  constexpr int NR = (HQ ? 1 : 0) + (HS ? 1 : 0) + (HB ? 1 : 0);
+  const int cap = std::max(1, bulk_max_pairs(op, RC));
+  const size_t smem = bulk_smem_bytes(RC, NR, (int)a.b, cap, sizeof(T));
+  require(op->bulk_err != nullptr, SMA_ERR_INTERNAL, "bulk family without its error flag");
+  SMA_CUDA(cudaFuncSetAttribute(bulk_kernel<T, V, G, HQ, HS, HB>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const unsigned grid = (unsigned)((op->n + RC - 1) / RC);
+  bulk_kernel<T, V, G, HQ, HS, HB><<<grid, kBulkThreads, smem, a.st>>>(
+      op->rowptr, op->colind, val, op->n, (int)a.b, a.Q, a.ldq, a.B1, a.B2, a.ldb, a.out, a.ldo,
+      (T)a.ck, (T)a.alpha, (T)a.beta, cap, op->bulk_err);
+  SMA_CHECK_LAUNCH();
+}
+
+// Whether the BULK family can take this step: whole rows of 16..512 bytes, every leading
+// dimension and base address on 16 bytes, and the largest CTA's rows within shared memory.
+template <typename T, bool HQ, bool HS, bool HB>
+bool bulk_fits(const Args<T> &a, int V) {
+  const int64_t rb = a.b * (int64_t)sizeof(T);
+  if (a.cseg || rb < 16 || rb > 512 || rb % 16 || a.b % V) return false;
+  const int64_t G = a.b / V;
+  if (G != 4 && G != 8 && G != 16 && G != 32) return false;
+  auto al = [](const void *p) { return p == nullptr || ((uintptr_t)p & 15) == 0; };
+  if ((a.ldb * sizeof(T)) % 16 || (HQ && (a.ldq * sizeof(T)) % 16) || !al(a.Q) || !al(a.B1) ||
+      !al(a.B2))
+    return false;
+  const int RC = kBulkThreads / (int)G;
+  const int nr = (HQ ? 1 : 0) + (HS ? 1 : 0) + (HB ? 1 : 0);
+  const int cap = std::max(1, bulk_max_pairs(a.op, RC));
+  return bulk_smem_bytes(RC, nr, (int)a.b, cap, sizeof(T)) <= 200 * 1024;
+}
+
 template <typename T, int V, bool HQ, bool HS, bool HB>
 void launch_v(int c, const Args<T> &a) {
   const int fam = fam_of(c);
+  if (fam == 3) {
+    switch (g_of(c)) {
+      case 4: return launch_bulk<T, V, 4, HQ, HS, HB>(a);
+      case 8: return launch_bulk<T, V, 8, HQ, HS, HB>(a);
+      case 16: return launch_bulk<T, V, 16, HQ, HS, HB>(a);
+      case 32: return launch_bulk<T, V, 32, HQ, HS, HB>(a);
+      default: throw Error(SMA_ERR_INTERNAL, "bad bulk CSR kernel configuration");
+    }
+  }
   if (fam == 2) {
     if constexpr (V * sizeof(T) == 16) {
       switch (g_of(c) * 100 + u_of(c)) {
@@ -392,6 +600,16 @@ void step(const Args<T> &a) {
           tu.cands.push_back(enc(fam, V, G, 4));
         }
       }
+    for (int V : {vmax, vmax / 2}) {  // the BULK family: whole rows staged by bulk copies
+      // (a key with 16-byte vectors guarantees 16-byte pointers and leading dimensions)
+      if (V >= 1 && vmax * (int)sizeof(T) >= 16 && bulk_fits<T, HQ, HS, HB>(a, V)) {
+        if (!op->bulk_err) {
+          SMA_CUDA(cudaMalloc((void **)&const_cast<sma_op *>(op)->bulk_err, sizeof(int)));
+          SMA_CUDA(cudaMemset(op->bulk_err, 0, sizeof(int)));
+        }
+        tu.cands.push_back(enc(3, V, (int)(a.b / V), 0));
+      }
+    }
     if (vmax * (int)sizeof(T) >= 16 && !a.cseg) {  // the ASYNC family moves 16-byte chunks
       const int V = 16 / (int)sizeof(T);
       const int64_t lanes = (a.b + V - 1) / V;
@@ -434,7 +652,10 @@ void step(const Args<T> &a) {
             (long long)op->n, (long long)a.b, (long long)a.ldb, (int)HQ, (int)HS, (int)HB);
     for (size_t i = 0; i < ncand; ++i)
       fprintf(stderr, " %s%s/V%d/G%d/U%d=%.1fus", i == w ? "*" : "",
-              fam_of(tu.cands[i]) == 2 ? "async" : fam_of(tu.cands[i]) ? "staged" : "direct",
+              fam_of(tu.cands[i]) == 3   ? "bulk"
+              : fam_of(tu.cands[i]) == 2 ? "async"
+              : fam_of(tu.cands[i])      ? "staged"
+                                         : "direct",
               v_of(tu.cands[i]), g_of(tu.cands[i]), u_of(tu.cands[i]), 1e3 * best[i]);
     fprintf(stderr, "\n");
   }

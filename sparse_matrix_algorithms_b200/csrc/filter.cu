@@ -51,6 +51,19 @@ double clenshaw_step_bytes(const sma_op *op, int64_t b, int elem_bytes) {
   return mat + 4.0 * (double)op->n * (double)b * elem_bytes;
 }
 
+void check_bulk_error(const sma_op *op, cudaStream_t st) {
+  if (!op->bulk_err) return;
+  int h = 0;
+  SMA_CUDA(cudaMemcpyAsync(&h, op->bulk_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SMA_CUDA(cudaStreamSynchronize(st));
+  if (h != 0) {
+    SMA_CUDA(cudaMemsetAsync(op->bulk_err, 0, sizeof(int), st));
+    SMA_CUDA(cudaStreamSynchronize(st));
+    throw Error(SMA_ERR_TIMEOUT, h == 1 ? "a bulk-copy CSR step gave up waiting for its copies"
+                                        : "a bulk-copy CSR step met a CTA larger than its shared memory");
+  }
+}
+
 void op_apply(const sma_op *op, cudaStream_t st, const double *X, int64_t ldx, double *Y,
               int64_t ldy, int64_t b) {
   if (b == 0 || op->n == 0) return;
@@ -63,6 +76,7 @@ void op_apply(const sma_op *op, cudaStream_t st, const double *X, int64_t ldx, d
   }
   if (op->kind == OP_CSR_HALF) return half_product<double>(op, st, X, ldx, Y, ldy, b);
   launch_clenshaw_step<double>(op, st, b, nullptr, 0, X, nullptr, ldx, Y, ldy, 0.0, 1.0, 0.0, false);
+  check_bulk_error(op, st);
 }
 
 template <typename T>
@@ -146,9 +160,10 @@ static FilterCount record_filter(const sma_op *op, cudaStream_t st,
 constexpr int64_t kGraphMinDegree = 32;
 
 template <typename T>
-FilterCount apply_poly_block(const sma_op *op, cudaStream_t st, const std::vector<double> &coeffs,
-                             double smin, double smax, const T *Q, int64_t ldq, T *Y, int64_t ldy,
-                             int64_t b, ClenshawWork<T> &work) {
+static FilterCount apply_poly_block_impl(const sma_op *op, cudaStream_t st,
+                                         const std::vector<double> &coeffs, double smin,
+                                         double smax, const T *Q, int64_t ldq, T *Y, int64_t ldy,
+                                         int64_t b, ClenshawWork<T> &work) {
   FilterCount fc;
   const int64_t n = op->n;
   const int64_t K = (int64_t)coeffs.size() - 1;
@@ -214,6 +229,15 @@ FilterCount apply_poly_block(const sma_op *op, cudaStream_t st, const std::vecto
   g_kernel_launches.fetch_add(work.g_launches);
   work.replays += 1;
   launch_copy_block<T, T>(st, n, b, work.y.p, b, Y, ldy);
+  return fc;
+}
+
+template <typename T>
+FilterCount apply_poly_block(const sma_op *op, cudaStream_t st, const std::vector<double> &coeffs,
+                             double smin, double smax, const T *Q, int64_t ldq, T *Y, int64_t ldy,
+                             int64_t b, ClenshawWork<T> &work) {
+  const FilterCount fc = apply_poly_block_impl<T>(op, st, coeffs, smin, smax, Q, ldq, Y, ldy, b, work);
+  check_bulk_error(op, st);
   return fc;
 }
 

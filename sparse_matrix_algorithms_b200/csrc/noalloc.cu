@@ -124,6 +124,7 @@ void filter_noalloc(sma_op *op, const double *coeffs, int64_t K, double smin, do
     step(op, st, b, Q, ldq, B1, b2_zero ? nullptr : B2, Y, ldy, coeffs[0], invd, -(c * invd));
   }
   SMA_CUDA(cudaStreamSynchronize(st));
+  check_bulk_error(op, st);  // a tuned bulk-copy step reports a wait that gave up
 }
 
 }  // namespace

@@ -481,6 +481,7 @@ void batch_filter(const sma_op *op, cudaStream_t st, std::vector<std::unique_ptr
     columns += r * (int64_t)(w.coeffs.size() > 1 ? w.coeffs.size() - 1 : 1);
   }
   replays += b.run(use_graph);
+  check_bulk_error(op, st);
   const FilterCount fc = b.count();
   total.steps += fc.steps;
   total.bytes += fc.bytes;

@@ -135,6 +135,7 @@ FilterCount percol_filter(const sma_op *op, cudaStream_t st, const T *coef, int6
     TMP = t;
   }
   step(coef, Y, invd, -(c * invd));
+  check_bulk_error(op, st);
   fc.steps = K + 1;
   fc.bytes = (double)(K + 1) * (mat_bytes + 4 * blk);
   return fc;

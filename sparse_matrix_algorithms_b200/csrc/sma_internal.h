@@ -134,6 +134,12 @@ struct sma_op {
   void *user = nullptr;
   // autotuned CSR kernel configurations
   std::map<uint64_t, sma::CsrTune> tuned;
+  // BULK family of the CSR step (csr_clenshaw.cuh): the most CSR entries any CTA of RC rows
+  // holds, per RC (from a host copy of the row pointers), and the device flag its bounded
+  // wait sets when it gives up
+  std::map<int, int> bulk_pairs;
+  std::vector<int> host_rowptr;
+  int *bulk_err = nullptr;
   // matrix-free model stencils
   sma_stencil stencil;
 };
@@ -190,6 +196,9 @@ template <typename T>
 void csr_clenshaw_step(const sma_op *op, cudaStream_t st, int64_t b, const T *Q, int64_t ldq,
                        const T *B1, const T *B2, int64_t ldb, T *out, int64_t ldo, double ck,
                        double alpha, double beta, bool has_self);
+// Throws SMA_ERR_TIMEOUT (and clears the flag) when a BULK-family launch of the CSR step on
+// this operator gave up its bounded wait; synchronizes the stream when the family was used.
+void check_bulk_error(const sma_op *op, cudaStream_t st);
 // The CSR step without the autotuner (cached or default configuration, no events).
 template <typename T>
 void csr_clenshaw_step_untuned(const sma_op *op, cudaStream_t st, int64_t b, const T *Q,

@@ -226,3 +226,24 @@ def test_invalid_csr_is_rejected_before_upload(lib_built):
     assert rc == L.SMA_ERR_ARG
     with pytest.raises(S.ArgumentError):
         S.SparseOperator(sp.csr_matrix(np.array([[1.0, 2.0], [0.0, 1.0]])), check_symmetric=True)
+
+
+@pytest.mark.parametrize("precision,b", [("fp64", 32), ("fp64", 64), ("fp32", 64), ("fp32", 128)])
+def test_autotuned_filter_bit_identical_to_untuned(lib_built, monkeypatch, capfd, precision, b):
+    """The autotuner's trial steps run every candidate family on real recurrence steps --
+    DIRECT, STAGED, ASYNC and BULK (rows staged by bulk copies onto an mbarrier) -- so a tuned
+    filter equals an untuned one bit for bit only if every family computes the same bits.
+    The BULK family must have been among the candidates."""
+    import sparse_matrix_algorithms_b200 as S
+
+    A = M.anderson3d(30, 16.5, 9)  # n = 27000: autotuned
+    smin, smax = _bounds(A)
+    Q = M.splitmix_normal(3, A.shape[0], b)
+    c = O.build_coeffs(120, smin, smax, 0.0, -0.3, 0.3, "step", True)
+    monkeypatch.setenv("SMA_AUTOTUNE_VERBOSE", "1")
+    tuned = S.apply_poly_block(S.SparseOperator(A, S.Context(0)), Q, c, smin, smax, precision=precision)
+    err = capfd.readouterr().err
+    assert "bulk/" in err, err
+    monkeypatch.setenv("SMA_AUTOTUNE", "0")
+    plain = S.apply_poly_block(S.SparseOperator(A, S.Context(0)), Q, c, smin, smax, precision=precision)
+    np.testing.assert_array_equal(tuned, plain)
