@@ -195,8 +195,10 @@ def arm_pipeline(wl, op, net, precision="mixed", stats=None, report=None, vector
     lo, hi = S.lanczos_bounds(op, steps=LANCZOS_STEPS)
     mu = S.kpm_moments(op, P.N_MOMENTS, 16, smin=lo, smax=hi)
     rep = {}
+    # the acceptance criterion is relative: ||Ax - lam x|| <= 1e-10 ||A||, ||A|| from the bounds
+    tol = 1e-10 * max(abs(lo), abs(hi))
     lam, X, res, _ = P.solve_polfed_windows(op, [(wl.emin, wl.emax)], net, s=wl.s, smin=lo,
-                                            smax=hi, mu=mu, report=rep, stats=stats,
+                                            smax=hi, mu=mu, tol=tol, report=rep, stats=stats,
                                             precision=precision, vectors=vectors)
     if stats is not None:
         stats["plan"] = list(rep["plan"][0])
@@ -610,7 +612,8 @@ def run_multi(args):
         mu = S.kpm_moments(op, P.N_MOMENTS, 16, smin=l2, smax=h2)
         rep, st = {}, {}
         r = P.solve_polfed_windows(op, wins, net, s=s, smin=l2, smax=h2, mu=mu,
-                                   precision=args.precision, report=rep, stats=st, vectors=False)
+                                   precision=args.precision, tol=1e-10 * max(abs(l2), abs(h2)),
+                                   report=rep, stats=st, vectors=False)
         return r, rep, st
 
     ((lam, _, res, win), rep, st), t_pipe = timed(pipeline)

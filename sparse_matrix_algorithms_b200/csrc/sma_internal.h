@@ -399,11 +399,11 @@ using PolishTrace =
 using PolishNeeds = std::function<bool(double, double)>;
 // Polish settings, from the environment: SMA_POLISH_FILTER=step (an undamped step window
 // over the guards' span) or same (the basis filter, default); SMA_POLISH_GUARDS (guards as a
-// fraction of the in-window candidates, default 0.5); SMA_POLISH_DEGREE (degree scale of the
+// fraction of the in-window candidates, default 1); SMA_POLISH_DEGREE (degree scale of the
 // polish polynomial, default 1); SMA_POLISH_PASSES (default 3); SMA_POLISH_VERBOSE=1.
 struct PolishConfig {
   bool step_filter = false;
-  double guard_fraction = 0.5;
+  double guard_fraction = 1.0;
   double degree_scale = 1.0;
   int64_t max_passes = 3;
   bool verbose = false;

@@ -436,13 +436,15 @@ def plan_polfed_windows(A, windows, planner: Optional[WindowPlanner], *, s: int,
 
 def solve_polfed_windows(A, windows, planner: Optional[WindowPlanner] = None, *, s: int = 8,
                          smin=None, smax=None, mu=None, seed: int = 1,
-                         precision: str = "fp64", report: Optional[dict] = None,
-                         stats: Optional[dict] = None, vectors: bool = True):
+                         precision: str = "fp64", tol: float = 1e-10,
+                         report: Optional[dict] = None, stats: Optional[dict] = None,
+                         vectors: bool = True):
     """Batched POLFED over ``windows`` with a planned (nev, degree, mmax) per window (the
     learned plan when a planner is given, else the plain rule), all windows in one
     :func:`polfed_windows` call.  Every window whose learned plan returns fewer than
     0.85 N - 3 converged in-window pairs (N its KPM count) is solved again with the plain
-    rule (the redone windows batched together).  Returns ``(lam, X, res, win)``;
+    rule (the redone windows batched together).  ``tol`` is polfed's residual tolerance
+    (its return rule, and where a MIXED polish may stop).  Returns ``(lam, X, res, win)``;
     ``report`` receives the plans, the plain rule, the column-steps spent and the windows
     redone."""
     from .api import polfed_windows
@@ -460,7 +462,7 @@ def solve_polfed_windows(A, windows, planner: Optional[WindowPlanner] = None, *,
     def run(ws, pl, st):
         return polfed_windows(op, [windows[w] for w in ws], [p[0] for p in pl], [p[1] for p in pl],
                               [p[2] for p in pl], s=s, smin=smin, smax=smax, window_type="delta",
-                              seed=seed, precision=precision, stats=st, vectors=vectors)
+                              seed=seed, precision=precision, tol=tol, stats=st, vectors=vectors)
 
     ids = list(range(len(windows)))
     lam, X, res, win = run(ids, plans, stats)

@@ -198,8 +198,11 @@ def evaluate_polfed(weights=P.POLFED_WEIGHTS, problems=HELD_OUT_POLFED, counts=(
             gp = np.sort(lp[sp][(lp[sp] >= win[0]) & (lp[sp] <= win[1]) & (resp[sp] <= 1e-10 * nrm)])
             gl = np.sort(ll[sl][(ll[sl] >= win[0]) & (ll[sl] <= win[1]) & (resl[sl] <= 1e-10 * nrm)])
             same = gp.size == gl.size and (gp.size == 0 or float(np.abs(gp - gl).max()) <= 1e-12 * nrm)
+            # every pair the plain rule converged, the learned plan converged too (to 1e-12 ||A||)
+            covers = all(gl.size and float(np.abs(gl - x).min()) <= 1e-12 * nrm for x in gp)
             row = dict(problem=f"{kind} L={L} p={p} seed={seed}", window=win, plain=rp["cost"][w],
-                       learned=rl["cost"][w], redone=w in rl["redone"], same=same, found=int(gp.size),
+                       learned=rl["cost"][w], redone=w in rl["redone"], same=same, covers=covers,
+                       found=int(gp.size), found_learned=int(gl.size),
                        plain_plan=rp["plan"][w], learned_plan=rl["plan"][w])
             rows.append(row)
             if verbose:
