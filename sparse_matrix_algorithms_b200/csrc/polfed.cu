@@ -193,6 +193,8 @@ class PolfedWindow {
     X_.alloc(n * std::max<int64_t>(m, 1), st_);
     AX_.alloc(n * std::max<int64_t>(m, 1), st_);
     dn_.mul_small(n, M, m, V_.p, Mcap, Usel.p, M, X_.p, m, 1.0, 0.0);
+    V_.release();  // the basis is dead once the Ritz vectors are lifted (stream-ordered free)
+    T_.release();
     RitzSet rs = rayleigh(op_, st_, n, m, X_.p, m, AX_.p, lam_d_, res_d_, scratch_);
     std::vector<double> lam_keep, res_keep;
     std::vector<int64_t> idx_keep;
@@ -267,7 +269,9 @@ class PolfedWindow {
       if (colmap.empty()) return empty();
       Xfin = X_.p;
       ldfin = k;
+      Xc_.release();  // the refined vectors live in X_ now
     }
+    AX_.release();
     clk.close();
     if (o.precision == SMA_PREC_MIXED) {
       // FP64 polish of the FP32-filtered basis (polish.cu): filtered subspace iterations
@@ -285,6 +289,7 @@ class PolfedWindow {
         launch_copy_block<double, double>(st_, n, kin, Yp.p, kin, Xpol_.p, k);
         if (ng > 0) launch_copy_block<double, double>(st_, n, ng, guard.p, ng, Xpol_.p + kin, k);
       }
+      guard.release();
       auto done = [&](const std::vector<double> &lam, const std::vector<double> &res) {
         std::vector<double> r;
         for (size_t i = 0; i < lam.size(); ++i)
