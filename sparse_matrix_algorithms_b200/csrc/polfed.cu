@@ -309,8 +309,11 @@ class PolfedWindow {
       else if (Kp != (int64_t)coeffs.size() - 1)
         pcoef = build_coeffs(Kp, o.smin, o.smax, o.sigma, o.emin, o.emax, o.window_type,
                              o.jackson != 0);
-      auto needs = [&](double lam, double res) {  // guards and unconverged in-window pairs
-        return !(o.emin <= lam && lam <= o.emax) || res >= 0.5 * o.tol;
+      // after the first pass only unconverged in-window pairs are filtered again: what is
+      // left of their error lies beyond the guards' span, where re-filtering the guards
+      // does not reach; the guards keep their first-pass vectors in the Rayleigh-Ritz
+      auto needs = [&](double lam, double res) {
+        return o.emin <= lam && lam <= o.emax && res >= 0.5 * o.tol;
       };
       PolishTrace trace;
       if (pc.verbose)
