@@ -66,3 +66,34 @@ def test_half_storage_errors(lib_built):
         S.slice_spectrum(S.SparseOperator(A, storage="upper"), [(-0.1, 0.1)], [100], [16])
     with pytest.raises(S.ArgumentError):
         S.SparseOperator(A, storage="lower")
+
+
+def test_half_storage_applies_lower_triangle_and_its_bounds(lib_built):
+    """Half storage keeps the entries a_ij with i >= j of the CSC arrays (row i, column j),
+    so the operator applied is L + L^T - D (L = tril(A), D its diagonal) whatever the other
+    triangle held.  With check_symmetric off and a non-symmetric input, its products are
+    those of L + L^T - D and its Gershgorin bounds are L + L^T - D's, which enclose that
+    operator's spectrum."""
+    import sparse_matrix_algorithms_b200 as S
+
+    rng = np.random.default_rng(5)
+    n = 700
+    A = sp.random(n, n, density=0.01, random_state=5, format="csr") + sp.diags(rng.uniform(-2, 2, n))
+    A = sp.csr_matrix(A)  # not symmetric
+    L = sp.tril(A).tocsr()
+    Aapp = (L + L.T - sp.diags(A.diagonal())).tocsr()
+    half = S.SparseOperator(A, storage="upper")
+    d = Aapp.diagonal()
+    r = np.asarray(abs(Aapp).sum(axis=1)).ravel() - np.abs(d)
+    lo, hi = half.gershgorin_bounds()
+    assert lo == pytest.approx(float(np.min(d - r)), rel=1e-13, abs=1e-13)
+    assert hi == pytest.approx(float(np.max(d + r)), rel=1e-13, abs=1e-13)
+    ev = np.linalg.eigvalsh(Aapp.toarray())
+    assert lo <= ev[0] and ev[-1] <= hi
+    Q = M.splitmix_normal(2, n, 8)
+    c = np.zeros(2)
+    c[1] = 1.0  # p = T_1: Y = A_hat Q, which exposes the operator applied
+    Y = S.apply_poly_block(half, Q, c, lo, hi)
+    cen, dd = 0.5 * (lo + hi), 0.5 * (hi - lo)
+    ref = (Aapp @ Q - cen * Q) / dd
+    assert np.abs(Y - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
