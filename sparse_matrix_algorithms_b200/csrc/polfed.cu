@@ -298,17 +298,19 @@ class PolfedWindow {
         std::sort(r.begin(), r.end());
         return r[std::min<size_t>(nev, r.size()) - 1] < o.tol;
       };
-      // the polish polynomial: the basis filter, or an undamped step over the window
-      // widened to the guards' span (sharper edges: the guards take the transition)
-      std::vector<double> pcoef = coeffs;
+      // the polish polynomial of degree K: the basis filter's window, or an undamped step
+      // over the window widened to the guards' span (sharper edges: the guards take the
+      // transition); it starts at the basis degree (times SMA_POLISH_DEGREE) and may double
+      // twice when a pass stalls
+      auto coeffs_of = [&](int64_t K) {
+        if (pc.step_filter)
+          return build_coeffs(K, o.smin, o.smax, 0.5 * (guard_lo + guard_hi), guard_lo, guard_hi,
+                              SMA_WINDOW_STEP, false);
+        return build_coeffs(K, o.smin, o.smax, o.sigma, o.emin, o.emax, o.window_type,
+                            o.jackson != 0);
+      };
       const int64_t Kp = std::max<int64_t>(
           1, (int64_t)std::llround(pc.degree_scale * (double)(coeffs.size() - 1)));
-      if (pc.step_filter)
-        pcoef = build_coeffs(Kp, o.smin, o.smax, 0.5 * (guard_lo + guard_hi), guard_lo, guard_hi,
-                             SMA_WINDOW_STEP, false);
-      else if (Kp != (int64_t)coeffs.size() - 1)
-        pcoef = build_coeffs(Kp, o.smin, o.smax, o.sigma, o.emin, o.emax, o.window_type,
-                             o.jackson != 0);
       // after the first pass only unconverged in-window pairs are filtered again: what is
       // left of their error lies beyond the guards' span, where re-filtering the guards
       // does not reach; the guards keep their first-pass vectors in the Rayleigh-Ritz
@@ -330,8 +332,9 @@ class PolfedWindow {
                   (long long)pass, (long long)k, (long long)in, (long long)ok, mx);
         };
       clk.mark(PH_FILTER);
-      const PolishOut po = polish_mixed(op_, pcoef, o.smin, o.smax, Xpol_.p, k, done, needs,
-                                        pc.max_passes, polish, &stats.qr_fallbacks, trace);
+      const PolishOut po = polish_mixed(op_, coeffs_of, Kp, 4 * Kp, o.smin, o.smax, Xpol_.p, k,
+                                        done, needs, pc.max_passes, polish, &stats.qr_fallbacks,
+                                        trace);
       clk.close();
       stats.polish_iterations += po.passes;
       // keep the in-window pairs, as the refinement does

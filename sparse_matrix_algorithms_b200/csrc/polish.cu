@@ -175,23 +175,24 @@ PolishConfig polish_config() {
   return c;
 }
 
-PolishOut polish_mixed(const sma_op *op, const std::vector<double> &coeffs, double smin,
-                       double smax, double *X, int64_t k, const PolishDone &done,
+PolishOut polish_mixed(const sma_op *op, const PolishCoeffs &coeffs_of, int64_t K0, int64_t Kmax,
+                       double smin, double smax, double *X, int64_t k, const PolishDone &done,
                        const PolishNeeds &needs, int64_t max_passes, FilterCount &fc,
                        int64_t *qr_fallbacks, const PolishTrace &trace) {
   PolishOut out;
   sma_ctx *ctx = op->ctx;
   cudaStream_t st = ctx->stream;
   const int64_t n = op->n;
-  const int64_t K = (int64_t)coeffs.size() - 1;
-  require(K >= 1, SMA_ERR_ARG, "the polish needs a filter of degree >= 1");
+  require(K0 >= 1 && Kmax >= K0, SMA_ERR_ARG, "the polish needs a filter of degree >= 1");
+  int64_t K = K0;
+  std::vector<double> coeffs = coeffs_of(K);
   const double c = 0.5 * (smin + smax), d = 0.5 * (smax - smin);
   const int64_t kpad = (k + 7) / 8 * 8;  // FP32 rows of 32-byte multiples: full vector width
   Dense dn(ctx);
   DevBuf<double> AX(n * k, st), Y(n * k, st), H(k * k, st), mu(k, st), lam_d(k, st), res_d(k, st),
       scratch, theta_d(k, st), inv_s_d(k, st), pt_d(k, st), sd_d(k, st);
   DevBuf<float> R32(n * kpad, st), Z32(n * kpad, st), B1(n * kpad, st), B2(n * kpad, st),
-      TMP(n * kpad, st), AX32, coef32(K * kpad, st);
+      TMP(n * kpad, st), AX32, coef32(Kmax * kpad, st);
   if (op->kind != OP_CSR) AX32.alloc(n * kpad, st);
   DevBuf<int> colseg(kpad, st), act_d(kpad, st), slot_d(k, st);
   {
@@ -218,10 +219,19 @@ PolishOut polish_mixed(const sma_op *op, const std::vector<double> &coeffs, doub
   SMA_CUDA(cudaMemcpyAsync(Y.p, X, n * k * sizeof(double), cudaMemcpyDeviceToDevice, st));
   rayleigh_ritz(Y.p);
   if (trace) trace(0, out.lam, out.res);
-  std::vector<double> inv_s(k), pt(k), sd(k), e(K);
+  std::vector<double> inv_s(k), pt(k), sd(k), e;
   std::vector<float> cf;
   std::vector<int> act, slot(k);
+  // the largest residual among the columns still to converge
+  auto worst = [&]() {
+    double w = 0.0;
+    for (int64_t j = 0; j < k; ++j)
+      if (needs(out.lam[j], out.res[j])) w = std::max(w, out.res[j]);
+    return w;
+  };
+  double prev = worst();
   for (int64_t pass = 0; pass < max_passes && !done(out.lam, out.res); ++pass) {
+    e.resize(K);
     // the columns to filter: all of them in the first pass, then those the caller still needs
     act.clear();
     for (int64_t j = 0; j < k; ++j) {
@@ -261,7 +271,16 @@ PolishOut polish_mixed(const sma_op *op, const std::vector<double> &coeffs, doub
     SMA_CUDA(cudaStreamSynchronize(st));  // the host tables above are rewritten next pass
     out.passes += 1;
     out.columns += ka;
+    out.degree = K;
     if (trace) trace(out.passes, out.lam, out.res);
+    // a pass that cut the worst unconverged residual by less than 3x met the filter's ratio
+    // just outside the window, not the FP32 floor: sharpen the polynomial for the next pass
+    const double now = worst();
+    if (pass > 0 && now > prev / 3.0 && K < Kmax) {
+      K = std::min(2 * K, Kmax);
+      coeffs = coeffs_of(K);
+    }
+    prev = now;
   }
   return out;
 }

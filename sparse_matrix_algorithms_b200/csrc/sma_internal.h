@@ -388,7 +388,10 @@ struct PolishOut {
   std::vector<double> lam, res;  // Ritz values (ascending) and residual norms of X
   int64_t passes = 0;
   int64_t columns = 0;  // columns filtered, summed over the passes
+  int64_t degree = 0;   // polish degree of the last pass
 };
+// coeffs_of(K): the polish polynomial of degree K (Chebyshev coefficients, K + 1 values).
+using PolishCoeffs = std::function<std::vector<double>(int64_t)>;
 // done(lam, res) ends the passes early; trace(pass, lam, res) sees every pass (pass 0: the
 // Rayleigh-Ritz of the candidates before any filtering); needs(lam, res): whether a column
 // is filtered again after the first pass (converged in-window columns pass through to the
@@ -400,12 +403,12 @@ using PolishNeeds = std::function<bool(double, double)>;
 // Polish settings, from the environment: SMA_POLISH_FILTER=step (an undamped step window
 // over the guards' span) or same (the basis filter, default); SMA_POLISH_GUARDS (guards as a
 // fraction of the in-window candidates, default 1); SMA_POLISH_DEGREE (degree scale of the
-// polish polynomial, default 1); SMA_POLISH_PASSES (default 3); SMA_POLISH_VERBOSE=1.
+// polish polynomial, default 1); SMA_POLISH_PASSES (default 5); SMA_POLISH_VERBOSE=1.
 struct PolishConfig {
   bool step_filter = false;
   double guard_fraction = 1.0;
   double degree_scale = 1.0;
-  int64_t max_passes = 3;
+  int64_t max_passes = 5;
   bool verbose = false;
 };
 PolishConfig polish_config();
@@ -413,8 +416,10 @@ PolishConfig polish_config();
 // max_passes filtered subspace iterations with p = sum coeffs[m] T_m(A_hat), each applying
 // p as p(theta) x + q_theta(A_hat) r / d with q in FP32 (the first pass on every column,
 // later passes on the columns needs() selects); X ends as the last Ritz vectors.
-PolishOut polish_mixed(const sma_op *op, const std::vector<double> &coeffs, double smin,
-                       double smax, double *X, int64_t k, const PolishDone &done,
+// The degree starts at K0; after a pass (other than the first) that cut the worst unconverged
+// residual by less than 3x the next pass doubles it, up to Kmax.
+PolishOut polish_mixed(const sma_op *op, const PolishCoeffs &coeffs_of, int64_t K0, int64_t Kmax,
+                       double smin, double smax, double *X, int64_t k, const PolishDone &done,
                        const PolishNeeds &needs, int64_t max_passes, FilterCount &fc,
                        int64_t *qr_fallbacks, const PolishTrace &trace = PolishTrace());
 
