@@ -28,9 +28,11 @@ value      eigenpairs inside the window with relative residual ||Ax-lam x||/||A|
 e2e        the pipeline through the public API with host buffers: CSR upload, bounds, KPM,
            plan, solve and eigenvector download inside the timed region (host clock,
            device synchronized).
-roofline   the fused Clenshaw-SpMM step of the pipeline's filter: algorithmic bytes of all
-           its launches (nnz (s_v + 4) + 4 (n+1) + 4 n b s_x per step) over the device time
-           of the filter phases, against the measured HBM copy bandwidth.
+roofline   the fused Clenshaw-SpMM step of the pipeline's basis filter (one block shape,
+           b = s): algorithmic bytes of all its launches (nnz (s_v + 4) + 4 (n+1) + 4 n b s_x
+           per step) over the device time of the basis-filter phase, against the measured
+           HBM copy bandwidth.  The MIXED polish (ragged per-column widths, residual forms,
+           its own orthonormalization) is timed apart as polish_ms.
 cpu_baseline  the plain arm's POLFED configuration run by the CPU restatement of the
            reference (oracle/, FP64, OpenMP over the block's columns, all host threads) on a
            bounded sample: every block column, a truncated recurrence (its time scaled by
@@ -423,7 +425,8 @@ def run_ours(args, rank, world, device):
 
     def timed(name, fn, steps):
         pairs, ms, launches = 0, [], 0
-        agg = {"filter_bytes": 0.0, "filter_ms": 0.0, "orth_ms": 0.0, "rr_ms": 0.0}
+        agg = {"filter_bytes": 0.0, "filter_ms": 0.0, "orth_ms": 0.0, "rr_ms": 0.0,
+               "polish_ms": 0.0}
         for _ in range(steps):
             flush.zero_()
             torch.cuda.synchronize(device)
@@ -438,7 +441,7 @@ def run_ours(args, rank, world, device):
             ms.append(e0.elapsed_time(e1))
             pairs += wl.good_pairs(lam, res)
             for k in agg:
-                agg[k] += st[k]
+                agg[k] += st.get(k, 0.0)
             plans[name] = {k: st[k] for k in ("plan", "plain_rule", "redone", "polish_iterations",
                                               "fp32_filter_calls", "basis_dim") if k in st}
         step_ms[name] = [round(m, 1) for m in ms]
@@ -514,12 +517,13 @@ def run_ours(args, rank, world, device):
                        "pairs_per_step": t_pairs / arm_steps / world,
                        "over_plain": tuned_value / plain_value if plain_value > 0 else None},
         "plans": plans,
-        "phase_ms_per_step": {k: v_agg[k] / args.steps for k in ("filter_ms", "orth_ms", "rr_ms")},
+        "phase_ms_per_step": {k: v_agg[k] / args.steps
+                              for k in ("filter_ms", "orth_ms", "rr_ms", "polish_ms")},
         "step_ms": step_ms,
         "spmm_gbs": achieved,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": TRAFFIC.get((wl.name, args.precision)),
-                     "kernel": "fused CSR Clenshaw step (SpMM + recurrence axpy), all filter launches",
+                     "kernel": "fused CSR Clenshaw step (SpMM + recurrence axpy), the basis filter's launches",
                      "peak_kind": f"{peak_kind} HBM copy bandwidth",
                      "note": ("working set (~56 MB) is L2-resident at this size"
                               if wl.name == "c2" else "blocks of 67-134 MB per step exceed L2")},
@@ -622,7 +626,8 @@ def run_multi(args):
                        "eigenpairs_per_s": sum(g_pipe) / t_pipe, "plans": rep["plan"],
                        "plain_rule": rep["plain"], "redone": rep["redone"],
                        "filter_ms": st.get("filter_ms"), "orth_ms": st.get("orth_ms"),
-                       "rr_ms": st.get("rr_ms"), "polish_passes": st.get("polish_iterations"),
+                       "rr_ms": st.get("rr_ms"), "polish_ms": st.get("polish_ms"),
+                       "polish_passes": st.get("polish_iterations"),
                        "spmm_gbs": st["filter_bytes"] / st["filter_ms"] / 1e6 if st.get("filter_ms") else None}
     print(json.dumps(out), flush=True)
     if args.no_plain:

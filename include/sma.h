@@ -123,11 +123,12 @@ typedef struct sma_stats {
   int64_t basis_dim;      /* POLFED basis dimension M; Chebyshev m0 */
   int64_t spmm_steps;     /* block sparse products issued by the filter */
   int64_t spmm_columns;   /* sum over those products of the block width */
-  double filter_ms;       /* block Clenshaw filter */
+  double filter_ms;       /* block Clenshaw filter (the POLFED basis / Chebyshev iterations;
+                             the MIXED polish is counted in polish_ms) */
   double orth_ms;         /* orthogonalization / reorthogonalization */
   double rr_ms;           /* Rayleigh-Ritz, residuals, extraction */
   double total_ms;        /* whole solve, wall clock from call to return */
-  double filter_bytes;    /* algorithmic bytes of the filter's sparse products */
+  double filter_bytes;    /* algorithmic bytes of those filter products */
   int64_t qr_fallbacks;   /* blocks that left CholQR2 for shifted CholQR3 / Householder */
   int64_t warnings;       /* bit 0: interval outside the spectral bounds */
   int64_t kernel_launches; /* this library's own CUDA kernels launched by the solve
@@ -136,7 +137,9 @@ typedef struct sma_stats {
   int64_t locked;         /* pairs locked during the solve (Chebyshev with lock = 1) */
   int64_t polish_iterations; /* FP64 polishing iterations after an FP32 POLFED basis */
   int64_t graph_replays;  /* CUDA graph launches of the batched slicing filter */
-  int64_t reserved[3];
+  double polish_ms;       /* MIXED POLFED polish: filters, orthonormalization, Rayleigh-Ritz */
+  double polish_bytes;    /* algorithmic bytes of the polish's filter products */
+  int64_t reserved[1];
 } sma_stats;
 
 /* Options of batched spectrum slicing (sma_slice_solve); every window runs Chebyshev

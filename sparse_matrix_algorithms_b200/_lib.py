@@ -88,7 +88,8 @@ class Stats(ctypes.Structure):
                 ("qr_fallbacks", c_int64), ("warnings", c_int64), ("kernel_launches", c_int64),
                 ("fp32_filter_calls", c_int64), ("locked", c_int64),
                 ("polish_iterations", c_int64), ("graph_replays", c_int64),
-                ("reserved", c_int64 * 3)]
+                ("polish_ms", c_double), ("polish_bytes", c_double),
+                ("reserved", c_int64 * 1)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}

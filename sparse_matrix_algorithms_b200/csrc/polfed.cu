@@ -278,7 +278,7 @@ class PolfedWindow {
       // with the same polynomial on the in-window candidates plus the guard vectors, each
       // pass applying p as p(theta) x + q_theta(A_hat) r / d with the divided difference q
       // in FP32, then FP64 orthonormalization and Rayleigh-Ritz with A; until the best
-      // min(nev, in-window) residuals are below tol, at most three passes.
+      // min(nev, in-window) residuals are below tol, at most max_passes passes.
       const int64_t kin = (int64_t)colmap.size();
       const int64_t k = kin + ng;
       Xpol_.alloc(n * k, st_);
@@ -331,7 +331,7 @@ class PolfedWindow {
           fprintf(stderr, "polish pass %lld: k=%lld in-window=%lld converged=%lld max-res=%.3e\n",
                   (long long)pass, (long long)k, (long long)in, (long long)ok, mx);
         };
-      clk.mark(PH_FILTER);
+      clk.mark(PH_POLISH);
       const PolishOut po = polish_mixed(op_, coeffs_of, Kp, 4 * Kp, o.smin, o.smax, Xpol_.p, k,
                                         done, needs, pc.max_passes, polish, &stats.qr_fallbacks,
                                         trace);
@@ -406,16 +406,21 @@ class PolfedWindow {
   bool finished_ = false;
 };
 
-void fill_stats(sma_stats &stats, PhaseClock &clk, const FilterCount &fc, int64_t columns,
+// spmm_steps counts the basis filter's and the polish's products; filter_* and polish_*
+// keep the two apart (the basis filter runs one block shape, the polish ragged widths).
+void fill_stats(sma_stats &stats, PhaseClock &clk, const FilterCount &fc,
+                const FilterCount &polish, int64_t columns,
                 std::chrono::steady_clock::time_point t0, int64_t launches0) {
-  double ph[PH_COUNT] = {0, 0, 0};
+  double ph[PH_COUNT] = {0, 0, 0, 0};
   clk.totals(ph);
-  stats.spmm_steps = fc.steps;
+  stats.spmm_steps = fc.steps + polish.steps;
   stats.spmm_columns = columns;
   stats.filter_bytes = fc.bytes;
   stats.filter_ms = ph[PH_FILTER];
   stats.orth_ms = ph[PH_ORTH];
   stats.rr_ms = ph[PH_RR];
+  stats.polish_ms = ph[PH_POLISH];
+  stats.polish_bytes = polish.bytes;
   stats.total_ms = ms_since(t0);
   stats.kernel_launches = g_kernel_launches.load() - launches0;
 }
@@ -449,12 +454,11 @@ sma_result *polfed_solve(sma_op *op, int64_t nev, int64_t degree, const sma_polf
   stats.basis_dim = win.basis_dim();
   FilterCount polish;
   const WindowPairs wp = win.extract(clk, stats, polish);
-  flt.total.steps += polish.steps;
-  flt.total.bytes += polish.bytes;
   sma_result *r = wp.cols.empty() ? empty_result(ctx, op->n)
                                   : make_result(ctx, op->n, wp.X, wp.ldx, wp.cols, wp.lam, wp.res);
   const int64_t K = (int64_t)win.coeffs.size() - 1;
-  fill_stats(stats, clk, flt.total, flt.columns * std::max<int64_t>(K, 1), t0, launches0);
+  fill_stats(stats, clk, flt.total, polish, flt.columns * std::max<int64_t>(K, 1), t0,
+             launches0);
   stats.fp32_filter_calls = flt.fp32_calls + stats.polish_iterations;
   stats.graph_replays = flt.w64.replays + flt.w32.replays;
   r->stats = stats;
@@ -572,8 +576,6 @@ sma_result *polfed_batch_solve(sma_op *op, int64_t nwin, const double *emin, con
     pairs.push_back(w->extract(clk, stats, polish));
     k += (int64_t)pairs.back().cols.size();
   }
-  total.steps += polish.steps;
-  total.bytes += polish.bytes;
   sma_result *r;
   if (k == 0) {
     r = empty_result(ctx, n);
@@ -605,7 +607,7 @@ sma_result *polfed_batch_solve(sma_op *op, int64_t nwin, const double *emin, con
   }
   stats.iterations = blocks_max;
   stats.basis_dim = mdim;
-  fill_stats(stats, clk, total, columns, t0, launches0);
+  fill_stats(stats, clk, total, polish, columns, t0, launches0);
   stats.fp32_filter_calls = (fp32 ? calls : 0) + stats.polish_iterations;
   stats.graph_replays = replays;
   r->stats = stats;

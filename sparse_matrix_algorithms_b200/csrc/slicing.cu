@@ -188,7 +188,7 @@ sma_result *slice_solve(sma_op *op, int64_t nwin, const double *emin, const doub
       x.prev_ok = ok;
     }
   }
-  double ph[PH_COUNT] = {0, 0, 0};
+  double ph[PH_COUNT] = {0, 0, 0, 0};
   clk.totals(ph);
   // selection per window (chebyshev_subspace_iteration.jl:750-756), windows in order
   const double gate = std::max(o.res_gate, 10.0 * o.tol);

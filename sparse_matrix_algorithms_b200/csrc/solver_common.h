@@ -11,7 +11,7 @@
 namespace sma {
 namespace detail {
 
-enum Phase { PH_FILTER = 0, PH_ORTH = 1, PH_RR = 2, PH_COUNT = 3 };
+enum Phase { PH_FILTER = 0, PH_ORTH = 1, PH_RR = 2, PH_POLISH = 3, PH_COUNT = 4 };
 
 // Device time per phase from pairs of CUDA events on the solve's stream.
 struct PhaseClock {

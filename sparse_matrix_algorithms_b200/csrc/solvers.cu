@@ -107,7 +107,7 @@ sma_result *cheb_solve_locked(sma_op *op, double emin, double emax, const sma_ch
       launch_gather_columns_rm(st, n, m, X.p, m0, d.p, Q.p, m0);
     }
   }
-  double ph[PH_COUNT] = {0, 0, 0};
+  double ph[PH_COUNT] = {0, 0, 0, 0};
   clk.totals(ph);
   stats.iterations = it - 1;
   stats.basis_dim = m0;
@@ -289,7 +289,7 @@ sma_result *cheb_solve(sma_op *op, double emin, double emax, const sma_cheb_opts
       }
     }
   }
-  double ph[PH_COUNT] = {0, 0, 0};
+  double ph[PH_COUNT] = {0, 0, 0, 0};
   clk.totals(ph);
   stats.iterations = it - 1;
   stats.basis_dim = m0;

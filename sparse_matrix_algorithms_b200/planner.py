@@ -495,8 +495,9 @@ def solve_polfed_windows(A, windows, planner: Optional[WindowPlanner] = None, *,
         win = order_w[perm]
         X = np.concatenate(parts_x, axis=1)[:, perm] if parts_x else None
         if stats is not None:
-            for key in ("filter_ms", "orth_ms", "rr_ms", "filter_bytes", "spmm_steps",
-                        "spmm_columns", "kernel_launches", "polish_iterations"):
+            for key in ("filter_ms", "orth_ms", "rr_ms", "filter_bytes", "polish_ms",
+                        "polish_bytes", "spmm_steps", "spmm_columns", "kernel_launches",
+                        "polish_iterations"):
                 if key in st2:
                     stats[key] = stats.get(key, 0) + st2[key]
     if report is not None:
