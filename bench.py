@@ -714,6 +714,31 @@ def run_profile_orth(args):
                       "filter_ms": st["filter_ms"], "basis_dim": st["basis_dim"]}), flush=True)
 
 
+def run_profile_pipeline(args):
+    """One solve of the value arm (the pipeline) on the workload after its set-up (matrix
+    upload, Lanczos bounds for the norm): the command for ncu launch lists of a whole
+    pipeline solve.  Prints the solve's phase times and pairs."""
+    import torch
+
+    import sparse_matrix_algorithms_b200 as S
+    from sparse_matrix_algorithms_b200 import planner as P
+
+    wl = Workload(args.workload)
+    ctx = S.context(0)
+    op = S.SparseOperator(wl.A, ctx)
+    if wl.norm is None:
+        lo, hi = S.lanczos_bounds(op, steps=LANCZOS_STEPS)
+        wl.norm = max(abs(lo), abs(hi))
+    net = P.WindowPlanner.load(P.POLFED_WEIGHTS)
+    st = {}
+    lam, _, res = arm_pipeline(wl, op, net, args.precision, stats=st)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_pipeline": wl.name, "precision": args.precision,
+                      "pairs": wl.good_pairs(lam, res),
+                      **{k: st[k] for k in ("filter_ms", "orth_ms", "rr_ms", "polish_ms", "plan",
+                                            "kernel_launches") if k in st}}), flush=True)
+
+
 def run_profile_slice(args):
     """One iteration of batched slicing on the C3 matrix: four windows around E=0 with
     degrees 400/300/200/100 and widths 256/192/192/128 (768 columns at the top degree),
@@ -751,6 +776,8 @@ def main():
                     help="run only the Clenshaw filter of the workload (for ncu captures)")
     ap.add_argument("--profile-orth", action="store_true",
                     help="a short C3 POLFED solve for ncu captures of its GEMMs")
+    ap.add_argument("--profile-pipeline", action="store_true",
+                    help="one pipeline solve of the workload (for ncu launch lists)")
     ap.add_argument("--profile-slice", action="store_true",
                     help="one batched slicing iteration on the C3 matrix for ncu captures")
     ap.add_argument("--width", type=int, default=0, help="block width (default: the workload's s)")
@@ -762,6 +789,9 @@ def main():
         return
     if args.profile_orth:
         run_profile_orth(args)
+        return
+    if args.profile_pipeline:
+        run_profile_pipeline(args)
         return
     if args.profile_slice:
         run_profile_slice(args)

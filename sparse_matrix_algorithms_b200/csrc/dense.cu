@@ -71,6 +71,24 @@ void Dense::syevd(int64_t k, double *A, int64_t lda, double *w_dev, bool uplo_up
   require(h == 0, SMA_ERR_INTERNAL, "cusolverDnDsyevd failed, info=" + std::to_string(h));
 }
 
+bool Dense::sygvd(int64_t k, double *A, int64_t lda, double *B, int64_t ldb, double *w_dev) {
+  if (k == 0) return true;
+  int lwork = 0;
+  SMA_CUSOLVER(cusolverDnDsygvd_bufferSize(ctx->cusolver, CUSOLVER_EIG_TYPE_1,
+                                           CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                           (int)k, A, (int)lda, B, (int)ldb, w_dev, &lwork));
+  DevBuf<double> work(std::max(lwork, 1), ctx->stream);
+  DevBuf<int> info(1, ctx->stream);
+  SMA_CUSOLVER(cusolverDnDsygvd(ctx->cusolver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+                                CUBLAS_FILL_MODE_LOWER, (int)k, A, (int)lda, B, (int)ldb, w_dev,
+                                work.p, lwork, info.p));
+  int h = 0;
+  SMA_CUDA(cudaMemcpyAsync(&h, info.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  SMA_CUDA(cudaStreamSynchronize(ctx->stream));
+  require(h >= 0, SMA_ERR_INTERNAL, "cusolverDnDsygvd: bad argument " + std::to_string(-h));
+  return h == 0;  // h > k: B is not positive definite; 0 < h <= k: no convergence
+}
+
 namespace {
 
 // Upper Cholesky of the k x k column-major G in place. Returns cuSOLVER's info.

@@ -178,7 +178,14 @@ class PolfedWindow {
     DevBuf<double> theta_d(M, st_);
     dn_.syevd(M, T_.p, Mcap, theta_d.p, true);  // eigen(T), ascending
     const std::vector<double> theta = dev_to_host(st_, theta_d.p, M);
-    const int64_t m = std::min<int64_t>(M, std::max<int64_t>(o.overextract * nev, nev + o.extra_keep));
+    // m0 candidates (polfed.jl:901); MIXED with unfiltered guards lifts up to
+    // guard_fraction * nev more Ritz vectors, further out in theta, as guards only
+    const PolishConfig pc = polish_config();
+    const int64_t m0 = std::min<int64_t>(M, std::max<int64_t>(o.overextract * nev, nev + o.extra_keep));
+    const int64_t m =
+        (o.precision == SMA_PREC_MIXED && !pc.filter_guards)
+            ? std::min<int64_t>(M, m0 + (int64_t)std::ceil(pc.guard_fraction * (double)nev))
+            : m0;
     // p = sortperm(theta; rev=true)[1:m]
     std::vector<int64_t> order(M);
     std::iota(order.begin(), order.end(), 0);
@@ -198,7 +205,7 @@ class PolfedWindow {
     RitzSet rs = rayleigh(op_, st_, n, m, X_.p, m, AX_.p, lam_d_, res_d_, scratch_);
     std::vector<double> lam_keep, res_keep;
     std::vector<int64_t> idx_keep;
-    for (int64_t jj = 0; jj < m; ++jj)
+    for (int64_t jj = 0; jj < m0; ++jj)
       if (o.emin <= rs.lam[jj] && rs.lam[jj] <= o.emax) {
         lam_keep.push_back(rs.lam[jj]);
         res_keep.push_back(rs.res[jj]);
@@ -211,16 +218,29 @@ class PolfedWindow {
     DevBuf<double> guard;
     int64_t ng = 0;
     double guard_lo = o.emin, guard_hi = o.emax;  // the span of the guards' Ritz values
-    const PolishConfig pc = polish_config();
+    std::vector<double> guard_lam, guard_res;      // their Rayleigh quotients and residuals
     if (o.precision == SMA_PREC_MIXED) {
       std::vector<int64_t> outw;
       const int64_t want =
           std::max<int64_t>(1, (int64_t)std::ceil(pc.guard_fraction * (double)idx_keep.size()));
+      // Unfiltered guards must be converged about as far as the candidates: a guard that
+      // mixes eigenvectors from both sides of the window has a part, orthogonal to the
+      // candidates, whose Rayleigh quotient may fall inside the window -- a spurious
+      // in-window Ritz pair.  Guards are therefore the out-of-window Ritz vectors, in theta
+      // order, with residual at most 10x the largest in-window candidate residual.
+      double gmax = INFINITY;
+      if (!pc.filter_guards) {
+        gmax = 0.0;
+        for (double r : res_keep) gmax = std::max(gmax, r);
+        gmax *= 10.0;
+      }
       for (int64_t jj = 0; jj < m && (int64_t)outw.size() < want; ++jj)
-        if (!(o.emin <= rs.lam[jj] && rs.lam[jj] <= o.emax)) {
+        if (!(o.emin <= rs.lam[jj] && rs.lam[jj] <= o.emax) && rs.res[jj] <= gmax) {
           outw.push_back(jj);
           guard_lo = std::min(guard_lo, rs.lam[jj]);
           guard_hi = std::max(guard_hi, rs.lam[jj]);
+          guard_lam.push_back(rs.lam[jj]);
+          guard_res.push_back(rs.res[jj]);
         }
       ng = (int64_t)outw.size();
       if (ng > 0) {
@@ -290,6 +310,8 @@ class PolfedWindow {
         if (ng > 0) launch_copy_block<double, double>(st_, n, ng, guard.p, ng, Xpol_.p + kin, k);
       }
       guard.release();
+      X_.release();  // the candidates live in Xpol_ now (X_ held the refined vectors)
+      Xc_.release();
       auto done = [&](const std::vector<double> &lam, const std::vector<double> &res) {
         std::vector<double> r;
         for (size_t i = 0; i < lam.size(); ++i)
@@ -332,9 +354,14 @@ class PolfedWindow {
                   (long long)pass, (long long)k, (long long)in, (long long)ok, mx);
         };
       clk.mark(PH_POLISH);
+      // each column's Rayleigh quotient and residual on entry: the candidates' from the
+      // refinement (or extraction), the guards' from the extraction
+      std::vector<double> lam0 = lamc, res0 = resc;
+      lam0.insert(lam0.end(), guard_lam.begin(), guard_lam.end());
+      res0.insert(res0.end(), guard_res.begin(), guard_res.end());
       const PolishOut po = polish_mixed(op_, coeffs_of, Kp, 4 * Kp, o.smin, o.smax, Xpol_.p, k,
                                         done, needs, pc.max_passes, polish, &stats.qr_fallbacks,
-                                        trace);
+                                        lam0, res0, pc.filter_guards, pc.verbose, trace);
       clk.close();
       stats.polish_iterations += po.passes;
       // keep the in-window pairs, as the refinement does

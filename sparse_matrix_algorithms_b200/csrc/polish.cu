@@ -25,6 +25,7 @@
 // FP64, orthonormalization (CholQR2) and Rayleigh-Ritz with A, all in FP64.  The reference's
 // only post-processing is Rayleigh-Ritz (refine_original_rr, polfed.jl:837-880); this
 // filtered pass is what an FP32 basis needs on top of it to reach its tolerance.
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <string>
@@ -168,6 +169,10 @@ using detail::dev_to_host;
 PolishConfig polish_config() {
   PolishConfig c;
   if (const char *f = std::getenv("SMA_POLISH_FILTER")) c.step_filter = std::string(f) == "step";
+  if (const char *f = std::getenv("SMA_POLISH_FILTER_GUARDS")) c.filter_guards = std::string(f) == "1";
+  // unfiltered guards: three times the in-window count, so that one pass converges C3-sized
+  // windows; filtered guards: as many as the in-window candidates
+  c.guard_fraction = c.filter_guards ? 1.0 : 3.0;
   if (const char *g = std::getenv("SMA_POLISH_GUARDS")) c.guard_fraction = std::max(0.0, std::atof(g));
   if (const char *d = std::getenv("SMA_POLISH_DEGREE")) c.degree_scale = std::max(0.05, std::atof(d));
   if (const char *p = std::getenv("SMA_POLISH_PASSES")) c.max_passes = std::max(0, std::atoi(p));
@@ -178,7 +183,9 @@ PolishConfig polish_config() {
 PolishOut polish_mixed(const sma_op *op, const PolishCoeffs &coeffs_of, int64_t K0, int64_t Kmax,
                        double smin, double smax, double *X, int64_t k, const PolishDone &done,
                        const PolishNeeds &needs, int64_t max_passes, FilterCount &fc,
-                       int64_t *qr_fallbacks, const PolishTrace &trace) {
+                       int64_t *qr_fallbacks, const std::vector<double> &lam0,
+                       const std::vector<double> &res0, bool filter_all, bool verbose,
+                       const PolishTrace &trace) {
   PolishOut out;
   sma_ctx *ctx = op->ctx;
   cudaStream_t st = ctx->stream;
@@ -191,9 +198,21 @@ PolishOut polish_mixed(const sma_op *op, const PolishCoeffs &coeffs_of, int64_t 
   Dense dn(ctx);
   DevBuf<double> AX(n * k, st), Y(n * k, st), H(k * k, st), mu(k, st), lam_d(k, st), res_d(k, st),
       scratch, theta_d(k, st), inv_s_d(k, st), pt_d(k, st), sd_d(k, st);
-  DevBuf<float> R32(n * kpad, st), Z32(n * kpad, st), B1(n * kpad, st), B2(n * kpad, st),
-      TMP(n * kpad, st), AX32, coef32(Kmax * kpad, st);
-  if (op->kind != OP_CSR) AX32.alloc(n * kpad, st);
+  // the FP32 recurrence blocks hold the filtered columns only (the guards are never
+  // filtered unless filter_all), sized by the first pass and grown if a later pass needs more
+  DevBuf<float> R32, Z32, B1, B2, TMP, AX32, coef32;
+  int64_t fcap = 0;
+  auto ensure_fp32 = [&](int64_t kap) {
+    if (kap <= fcap) return;
+    fcap = kap;
+    R32.alloc(n * kap, st);
+    Z32.alloc(n * kap, st);
+    B1.alloc(n * kap, st);
+    B2.alloc(n * kap, st);
+    TMP.alloc(n * kap, st);
+    coef32.alloc(Kmax * kap, st);
+    if (op->kind != OP_CSR) AX32.alloc(n * kap, st);
+  };
   DevBuf<int> colseg(kpad, st), act_d(kpad, st), slot_d(k, st);
   {
     std::vector<int> idn(kpad);
@@ -215,9 +234,52 @@ PolishOut polish_mixed(const sma_op *op, const PolishCoeffs &coeffs_of, int64_t 
     out.lam = dev_to_host(st, lam_d.p, k);
     out.res = dev_to_host(st, res_d.p, k);
   };
-  // consistent start: Rayleigh-Ritz on the candidates themselves
-  SMA_CUDA(cudaMemcpyAsync(Y.p, X, n * k * sizeof(double), cudaMemcpyDeviceToDevice, st));
-  rayleigh_ritz(Y.p);
+  // The same Rayleigh-Ritz without orthonormalizing V first: S = V^T V, H = V^T A V and
+  // the generalized eigenproblem H E = S E diag(mu), X = V E (S-orthonormal E, so X has
+  // orthonormal columns): three n k^2 products instead of the six of CholQR2 followed by
+  // Rayleigh-Ritz.  The columns of V (filtered candidates and Ritz vectors of the basis)
+  // are nearly orthogonal, so S is well conditioned; when it is not positive definite the
+  // orthonormalizing path runs instead.
+  DevBuf<double> S;
+  auto rayleigh_ritz_gen = [&](double *V) {
+    if (!S.p) S.alloc(k * k, st);
+    op_apply(op, st, V, k, AX.p, k, k);
+    dn.gram(n, k, k, V, k, V, k, S.p, k);
+    dn.gram(n, k, k, V, k, AX.p, k, H.p, k);
+    if (!dn.sygvd(k, H.p, k, S.p, k, mu.p)) {
+      if (qr_fallbacks) ++*qr_fallbacks;
+      rayleigh_ritz(V);
+      return;
+    }
+    dn.mul_small(n, k, k, V, k, H.p, k, X, k, 1.0, 0.0);
+    op_apply(op, st, X, k, AX.p, k, k);
+    column_reduce(st, 0, n, k, X, k, AX.p, k, nullptr, lam_d.p, scratch);
+    column_reduce(st, 1, n, k, X, k, AX.p, k, lam_d.p, res_d.p, scratch);
+    out.lam = dev_to_host(st, lam_d.p, k);
+    out.res = dev_to_host(st, res_d.p, k);
+  };
+  // phase times for the verbose trace (the stream is synchronized only then)
+  auto now_ms = [&]() {
+    if (!verbose) return 0.0;
+    SMA_CUDA(cudaStreamSynchronize(st));
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch()).count();
+  };
+  double t_mark = now_ms();
+  if (filter_all || lam0.size() != (size_t)k || res0.size() != (size_t)k) {
+    // consistent start: Rayleigh-Ritz on the columns themselves
+    SMA_CUDA(cudaMemcpyAsync(Y.p, X, n * k * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    rayleigh_ritz(Y.p);
+  } else {
+    out.lam = lam0;
+    out.res = res0;
+    op_apply(op, st, X, k, AX.p, k, k);  // the residual block of the first pass reads A X
+  }
+  if (verbose) {
+    const double t = now_ms();
+    fprintf(stderr, "polish start: k=%lld %.1f ms\n", (long long)k, t - t_mark);
+    t_mark = t;
+  }
   if (trace) trace(0, out.lam, out.res);
   std::vector<double> inv_s(k), pt(k), sd(k), e;
   std::vector<float> cf;
@@ -235,12 +297,13 @@ PolishOut polish_mixed(const sma_op *op, const PolishCoeffs &coeffs_of, int64_t 
     // the columns to filter: all of them in the first pass, then those the caller still needs
     act.clear();
     for (int64_t j = 0; j < k; ++j) {
-      const bool f = pass == 0 || needs(out.lam[j], out.res[j]);
+      const bool f = (pass == 0 && filter_all) || needs(out.lam[j], out.res[j]);
       slot[j] = f ? (int)act.size() : -1;
       if (f) act.push_back((int)j);
     }
     const int64_t ka = (int64_t)act.size(), kapad = (ka + 7) / 8 * 8;
     if (ka == 0) break;
+    ensure_fp32(kapad);
     cf.assign(K * kapad, 0.f);
     for (int64_t a = 0; a < ka; ++a) {
       const int64_t j = act[a];
@@ -267,8 +330,17 @@ PolishOut polish_mixed(const sma_op *op, const PolishCoeffs &coeffs_of, int64_t 
     combine_kernel<<<grid_of(n * k), 256, 0, st>>>(n, k, X, k, Z32.p, kapad, slot_d.p, pt_d.p,
                                                    sd_d.p, Y.p, k);
     SMA_CHECK_LAUNCH();
-    rayleigh_ritz(Y.p);
+    const double t_filt = now_ms();
+    if (filter_all) rayleigh_ritz(Y.p);
+    else rayleigh_ritz_gen(Y.p);
     SMA_CUDA(cudaStreamSynchronize(st));  // the host tables above are rewritten next pass
+    if (verbose) {
+      const double t = now_ms();
+      fprintf(stderr, "polish pass %lld: filtered %lld columns at degree %lld in %.1f ms, "
+              "Rayleigh-Ritz of %lld in %.1f ms\n", (long long)pass + 1, (long long)ka,
+              (long long)K, t_filt - t_mark, (long long)k, t - t_filt);
+      t_mark = t;
+    }
     out.passes += 1;
     out.columns += ka;
     out.degree = K;

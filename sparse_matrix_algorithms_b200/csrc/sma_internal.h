@@ -365,6 +365,10 @@ struct Dense {
   // Symmetric eigen-decomposition of a k x k column-major matrix in place (vectors
   // overwrite A, eigenvalues ascending in w_dev). uplo_upper selects the triangle read.
   void syevd(int64_t k, double *A, int64_t lda, double *w_dev, bool uplo_upper);
+  // Generalized symmetric-definite eigenproblem A E = B E diag(w) (k x k column-major, lower
+  // triangles read): E overwrites A (B-orthonormal), B its Cholesky factor, eigenvalues
+  // ascending in w_dev.  Returns false when B is not positive definite.
+  bool sygvd(int64_t k, double *A, int64_t lda, double *B, int64_t ldb, double *w_dev);
 };
 
 // Orthonormalize the columns of a row-major n x k block in place and return the
@@ -393,35 +397,43 @@ struct PolishOut {
 // coeffs_of(K): the polish polynomial of degree K (Chebyshev coefficients, K + 1 values).
 using PolishCoeffs = std::function<std::vector<double>(int64_t)>;
 // done(lam, res) ends the passes early; trace(pass, lam, res) sees every pass (pass 0: the
-// Rayleigh-Ritz of the candidates before any filtering); needs(lam, res): whether a column
-// is filtered again after the first pass (converged in-window columns pass through to the
-// Rayleigh-Ritz unchanged).
+// columns before any filtering); needs(lam, res): whether a column is filtered (converged
+// in-window columns and guards pass through to the Rayleigh-Ritz unchanged).
 using PolishDone = std::function<bool(const std::vector<double> &, const std::vector<double> &)>;
 using PolishTrace =
     std::function<void(int64_t, const std::vector<double> &, const std::vector<double> &)>;
 using PolishNeeds = std::function<bool(double, double)>;
 // Polish settings, from the environment: SMA_POLISH_FILTER=step (an undamped step window
 // over the guards' span) or same (the basis filter, default); SMA_POLISH_GUARDS (guards as a
-// fraction of the in-window candidates, default 1); SMA_POLISH_DEGREE (degree scale of the
+// fraction of the in-window candidates, default 3, or 1 with filtered guards);
+// SMA_POLISH_FILTER_GUARDS=1 (the first
+// pass filters the guards too, and a Rayleigh-Ritz of all columns precedes it; default 0:
+// guards enter the Rayleigh-Ritz unfiltered); SMA_POLISH_DEGREE (degree scale of the
 // polish polynomial, default 1); SMA_POLISH_PASSES (default 5); SMA_POLISH_VERBOSE=1.
 struct PolishConfig {
   bool step_filter = false;
-  double guard_fraction = 1.0;
+  double guard_fraction = 3.0;
+  bool filter_guards = false;
   double degree_scale = 1.0;
   int64_t max_passes = 5;
   bool verbose = false;
 };
 PolishConfig polish_config();
-// Rayleigh-Ritz with A on the k columns of X (n x k, ld k, FP64, in place), then up to
-// max_passes filtered subspace iterations with p = sum coeffs[m] T_m(A_hat), each applying
-// p as p(theta) x + q_theta(A_hat) r / d with q in FP32 (the first pass on every column,
-// later passes on the columns needs() selects); X ends as the last Ritz vectors.
+// Up to max_passes filtered subspace iterations on the k columns of X (n x k, ld k, FP64,
+// in place) with p = sum coeffs[m] T_m(A_hat), each applying p as
+// p(theta) x + q_theta(A_hat) r / d with q in FP32 to the columns needs() selects (with
+// filter_all, every column in the first pass), then FP64 orthonormalization and
+// Rayleigh-Ritz with A on all k columns; X ends as the last Ritz vectors.
+// lam0/res0: each column's Rayleigh quotient and residual norm on entry (its columns unit
+// vectors); when empty (or with filter_all), a Rayleigh-Ritz of the k columns comes first.
 // The degree starts at K0; after a pass (other than the first) that cut the worst unconverged
 // residual by less than 3x the next pass doubles it, up to Kmax.
 PolishOut polish_mixed(const sma_op *op, const PolishCoeffs &coeffs_of, int64_t K0, int64_t Kmax,
                        double smin, double smax, double *X, int64_t k, const PolishDone &done,
                        const PolishNeeds &needs, int64_t max_passes, FilterCount &fc,
-                       int64_t *qr_fallbacks, const PolishTrace &trace = PolishTrace());
+                       int64_t *qr_fallbacks, const std::vector<double> &lam0,
+                       const std::vector<double> &res0, bool filter_all, bool verbose,
+                       const PolishTrace &trace = PolishTrace());
 
 // ------------------------------------------------------------------ result
 }  // namespace sma
