@@ -28,6 +28,7 @@ struct SliceBatch {
   int64_t n = 0, W = 0, Kmax = 0;
   double smin = 0, smax = 0;
   DevBuf<T> coef;       // (Kmax + 1) x nseg: coef[k * nseg + s] = c_k of segment s (0 above K_s)
+  std::vector<double> coef1;  // one segment: its coefficients, for the unsegmented step
   DevBuf<int> colseg;  // W: the segment of every column
   DevBuf<T> q, y, b1, b2, tmp;
   std::vector<int64_t> active;  // active[k] = width of the columns taking part at index k
@@ -74,6 +75,9 @@ struct SliceBatch {
     for (int64_t k = 0; k <= Kmax; ++k)
       for (int64_t s = 0; s < nseg; ++s)
         if (deg[s] >= k) active[k] = off[s] + width[s];
+    coef1.clear();
+    if (nseg == 1)
+      for (int64_t k = 0; k <= Kmax; ++k) coef1.push_back((double)ch[k]);
     coef.alloc(ch.size(), st);
     colseg.alloc(cs.size(), st);
     SMA_CUDA(cudaMemcpyAsync(coef.p, ch.data(), ch.size() * sizeof(T), cudaMemcpyHostToDevice, st));
@@ -86,9 +90,25 @@ struct SliceBatch {
     SMA_CUDA(cudaStreamSynchronize(st));  // the host tables above must outlive their copies
   }
 
+  // One step at index k over the first b columns.  One segment: the unsegmented step with
+  // the scalar c_k (the same arithmetic on the same values -- (T) c_k either way -- without
+  // the per-column coefficient lookups); several: the segmented step.
+  void step(int64_t k, int64_t b, const T *B1, const T *B2, T *out, double al, double be,
+            bool tuned) {
+    const int64_t nseg = (int64_t)wins.size();
+    if (nseg == 1) {
+      if (tuned)
+        csr_clenshaw_step<T>(op, st, b, q.p, W, B1, B2, W, out, W, coef1[k], al, be, true);
+      else
+        csr_clenshaw_step_untuned<T>(op, st, b, q.p, W, B1, B2, W, out, W, coef1[k], al, be, true);
+      return;
+    }
+    csr_clenshaw_step_seg<T>(op, st, b, q.p, W, B1, B2, W, out, W, coef.p + k * nseg, colseg.p,
+                             al, be, tuned);
+  }
+
   // The whole recurrence on q -> y.  tuned = false for graph recording.
   void record(bool tuned) {
-    const int64_t nseg = (int64_t)wins.size();
     const double c = 0.5 * (smin + smax), invd = 2.0 / (smax - smin);
     const double alpha = 2.0 * invd, beta = -2.0 * c * invd;
     const size_t bytes = (size_t)(n * W) * sizeof(T);
@@ -97,15 +117,13 @@ struct SliceBatch {
     SMA_CUDA(cudaMemsetAsync(tmp.p, 0, bytes, st));
     T *B1 = b1.p, *B2 = b2.p, *TMP = tmp.p;
     for (int64_t k = Kmax; k >= 1; --k) {
-      csr_clenshaw_step_seg<T>(op, st, active[k], q.p, W, B1, B2, W, TMP, W, coef.p + k * nseg,
-                               colseg.p, alpha, beta, tuned);
+      step(k, active[k], B1, B2, TMP, alpha, beta, tuned);
       T *t = B2;
       B2 = B1;
       B1 = TMP;
       TMP = t;
     }
-    csr_clenshaw_step_seg<T>(op, st, W, q.p, W, B1, B2, W, y.p, W, coef.p, colseg.p, invd,
-                             -(c * invd), tuned);
+    step(0, W, B1, B2, y.p, invd, -(c * invd), tuned);
   }
 
   // Algorithmic bytes of one batched filter: every step reads the matrix once and Q, B1,
