@@ -196,13 +196,28 @@ class PolfedWindow {
       DevBuf<int64_t> d = upload_idx(st_, order);
       launch_gather_columns_cm(st_, M, m, T_.p, Mcap, d.p, Usel.p, M);
     }
-    // X = V Usel (build_X!), all m columns at once: chunking does not change the values
+    // X = V Usel (build_X!): the m0 candidates first (chunking does not change the values);
+    // the further Ritz vectors only as far as the guard search below needs them
     X_.alloc(n * std::max<int64_t>(m, 1), st_);
     AX_.alloc(n * std::max<int64_t>(m, 1), st_);
-    dn_.mul_small(n, M, m, V_.p, Mcap, Usel.p, M, X_.p, m, 1.0, 0.0);
-    V_.release();  // the basis is dead once the Ritz vectors are lifted (stream-ordered free)
-    T_.release();
-    RitzSet rs = rayleigh(op_, st_, n, m, X_.p, m, AX_.p, lam_d_, res_d_, scratch_);
+    dn_.mul_small(n, M, m0, V_.p, Mcap, Usel.p, M, X_.p, m, 1.0, 0.0);
+    RitzSet rs = rayleigh(op_, st_, n, m0, X_.p, m, AX_.p, lam_d_, res_d_, scratch_);
+    int64_t mdone = m0;
+    auto lift_more = [&](int64_t cnt) {
+      cnt = std::min(cnt, m - mdone);
+      if (cnt <= 0) return false;
+      dn_.mul_small(n, M, cnt, V_.p, Mcap, Usel.p + mdone * M, M, X_.p + mdone, m, 1.0, 0.0);
+      const RitzSet r2 = rayleigh(op_, st_, n, cnt, X_.p + mdone, m, AX_.p + mdone, lam_d_,
+                                  res_d_, scratch_);
+      rs.lam.insert(rs.lam.end(), r2.lam.begin(), r2.lam.end());
+      rs.res.insert(rs.res.end(), r2.res.begin(), r2.res.end());
+      mdone += cnt;
+      return true;
+    };
+    auto drop_basis = [&]() {  // the basis is dead once the Ritz vectors are lifted
+      V_.release();            // (stream-ordered frees)
+      T_.release();
+    };
     std::vector<double> lam_keep, res_keep;
     std::vector<int64_t> idx_keep;
     for (int64_t jj = 0; jj < m0; ++jj)
@@ -211,7 +226,10 @@ class PolfedWindow {
         res_keep.push_back(rs.res[jj]);
         idx_keep.push_back(jj);
       }
-    if (idx_keep.empty()) return empty();
+    if (idx_keep.empty()) {
+      drop_basis();
+      return empty();
+    }
     // MIXED: guard Ritz vectors for the polish, taken in theta order from the out-of-window
     // columns of X before the refinement reuses X's storage.  Without guards the polish
     // converges at the ratio p(first outside)/p(window edge), which is close to 1.
@@ -234,7 +252,8 @@ class PolfedWindow {
         for (double r : res_keep) gmax = std::max(gmax, r);
         gmax *= 10.0;
       }
-      for (int64_t jj = 0; jj < m && (int64_t)outw.size() < want; ++jj)
+      for (int64_t jj = 0; (int64_t)outw.size() < want; ++jj) {
+        if (jj >= mdone && !lift_more(5 * (want - (int64_t)outw.size()) / 4 + 64)) break;
         if (!(o.emin <= rs.lam[jj] && rs.lam[jj] <= o.emax) && rs.res[jj] <= gmax) {
           outw.push_back(jj);
           guard_lo = std::min(guard_lo, rs.lam[jj]);
@@ -242,6 +261,7 @@ class PolfedWindow {
           guard_lam.push_back(rs.lam[jj]);
           guard_res.push_back(rs.res[jj]);
         }
+      }
       ng = (int64_t)outw.size();
       if (ng > 0) {
         guard.alloc(n * ng, st_);
@@ -249,6 +269,7 @@ class PolfedWindow {
         launch_gather_columns_rm(st_, n, ng, X_.p, m, d.p, guard.p, ng);
       }
     }
+    drop_basis();
     const int64_t npre = std::min<int64_t>((int64_t)res_keep.size(), nev + o.extra_keep);
     std::vector<int64_t> ps0 = stable_argsort(res_keep);
     ps0.resize(npre);
@@ -264,7 +285,10 @@ class PolfedWindow {
     int64_t ldfin = npre;
     std::vector<int64_t> colmap(npre);
     std::iota(colmap.begin(), colmap.end(), 0);
-    if (o.refine) {
+    // MIXED with unfiltered guards: the polish's Rayleigh-Ritz (on the candidates, filtered,
+    // and the guards) takes the place of the refinement, which would only rotate the
+    // candidates among themselves first
+    if (o.refine && !(o.precision == SMA_PREC_MIXED && !pc.filter_guards)) {
       // refine_original_rr (polfed.jl:837-880); orth_block_polfed! at its default rtol=1e-12
       const int64_t k = orthonormalize(ctx_, n, npre, Xc_.p, npre, true, 1e-12, nullptr, &stats.qr_fallbacks);
       if (k == 0) return empty();
