@@ -26,10 +26,11 @@
 namespace sma {
 
 void Dense::gram(int64_t n, int64_t m, int64_t k, const double *X, int64_t ldx, const double *Y,
-                 int64_t ldy, double *C, int64_t ldc, double alpha, double beta) {
+                 int64_t ldy, double *C, int64_t ldc, double alpha, double beta, bool upper) {
   if (m == 0 || k == 0) return;
   if (!ctx->cublas_dense) {
-    dgemm_gram(ctx->stream, ctx->num_sms, n, m, k, X, ldx, Y, ldy, C, ldc, alpha, beta, work);
+    dgemm_gram(ctx->stream, ctx->num_sms, n, m, k, X, ldx, Y, ldy, C, ldc, alpha, beta, work,
+               upper && m == k);
     return;
   }
   SMA_CUBLAS(cublasDgemm(ctx->cublas, CUBLAS_OP_N, CUBLAS_OP_T, (int)m, (int)k, (int)n, &alpha, X,
@@ -75,12 +76,12 @@ bool Dense::sygvd(int64_t k, double *A, int64_t lda, double *B, int64_t ldb, dou
   if (k == 0) return true;
   int lwork = 0;
   SMA_CUSOLVER(cusolverDnDsygvd_bufferSize(ctx->cusolver, CUSOLVER_EIG_TYPE_1,
-                                           CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                           CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER,
                                            (int)k, A, (int)lda, B, (int)ldb, w_dev, &lwork));
   DevBuf<double> work(std::max(lwork, 1), ctx->stream);
   DevBuf<int> info(1, ctx->stream);
   SMA_CUSOLVER(cusolverDnDsygvd(ctx->cusolver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
-                                CUBLAS_FILL_MODE_LOWER, (int)k, A, (int)lda, B, (int)ldb, w_dev,
+                                CUBLAS_FILL_MODE_UPPER, (int)k, A, (int)lda, B, (int)ldb, w_dev,
                                 work.p, lwork, info.p));
   int h = 0;
   SMA_CUDA(cudaMemcpyAsync(&h, info.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));

@@ -172,7 +172,8 @@ struct GramSmem {
 __global__ void __launch_bounds__(kGramThreads)
 gram_partial_kernel(int64_t n, int m, int k, const double *__restrict__ X, int64_t ldx,
                     const double *__restrict__ Y, int64_t ldy, int64_t rows_per_split,
-                    double *__restrict__ part, bool vec16) {
+                    double *__restrict__ part, bool vec16, bool upper) {
+  if (upper && blockIdx.x > blockIdx.y) return;  // a tile below the diagonal (no barrier yet)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   GramSmem &sm = *reinterpret_cast<GramSmem *>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -258,12 +259,13 @@ gram_partial_kernel(int64_t n, int m, int k, const double *__restrict__ X, int64
 // C[i + j ldc] = alpha * sum_s part_s(i, j) + beta * C[i + j ldc], splits summed in order.
 __global__ void gram_reduce_kernel(int m, int k, int tiles_m, int tiles_k, int splits,
                                    const double *__restrict__ part, double *C, int64_t ldc,
-                                   double alpha, double beta) {
+                                   double alpha, double beta, bool upper) {
   const int64_t total = (int64_t)m * k;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
     const int i = (int)(e % m), j = (int)(e / m);
     const int bx = i / GM, by = j / GN, ii = i % GM, jj = j % GN;
+    if (upper && bx > by) continue;  // its partials were never written
     double s = 0.0;
     for (int z = 0; z < splits; ++z)
       s += part[(((int64_t)z * tiles_k + by) * tiles_m + bx) * (GM * GN) + ii + jj * GM];
@@ -300,7 +302,7 @@ void dgemm_update(cudaStream_t st, int num_sms, int64_t n, int64_t m, int64_t p,
 
 void dgemm_gram(cudaStream_t st, int num_sms, int64_t n, int64_t m, int64_t k, const double *X,
                 int64_t ldx, const double *Y, int64_t ldy, double *C, int64_t ldc, double alpha,
-                double beta, DevBuf<double> &work) {
+                double beta, DevBuf<double> &work, bool upper) {
   using namespace dmma;
   if (m == 0 || k == 0) return;
   require(m <= INT32_MAX && k <= INT32_MAX, SMA_ERR_ARG, "product too wide");
@@ -315,12 +317,12 @@ void dgemm_gram(cudaStream_t st, int num_sms, int64_t n, int64_t m, int64_t k, c
   const size_t smem = sizeof(GramSmem);
   SMA_CUDA(cudaFuncSetAttribute(gram_partial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   gram_partial_kernel<<<dim3(tm, tk, (unsigned)splits), kGramThreads, smem, st>>>(
-      n, (int)m, (int)k, X, ldx, Y, ldy, rows, work.p, vec16);
+      n, (int)m, (int)k, X, ldx, Y, ldy, rows, work.p, vec16, upper && m == k);
   SMA_CHECK_LAUNCH();
   const int64_t total = m * k;
   const int blocks = (int)std::min<int64_t>((total + 255) / 256, 4LL * num_sms);
   gram_reduce_kernel<<<blocks, 256, 0, st>>>((int)m, (int)k, tm, tk, (int)splits, work.p, C, ldc,
-                                             alpha, beta);
+                                             alpha, beta, upper && m == k);
   SMA_CHECK_LAUNCH();
 }
 

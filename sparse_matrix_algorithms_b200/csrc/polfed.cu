@@ -385,7 +385,8 @@ class PolfedWindow {
       res0.insert(res0.end(), guard_res.begin(), guard_res.end());
       const PolishOut po = polish_mixed(op_, coeffs_of, Kp, 4 * Kp, o.smin, o.smax, Xpol_.p, k,
                                         done, needs, pc.max_passes, polish, &stats.qr_fallbacks,
-                                        lam0, res0, pc.filter_guards, pc.verbose, trace);
+                                        lam0, res0, o.emin, o.emax, pc.filter_guards,
+                                        pc.verbose, trace);
       clk.close();
       stats.polish_iterations += po.passes;
       // keep the in-window pairs, as the refinement does

@@ -184,8 +184,8 @@ PolishOut polish_mixed(const sma_op *op, const PolishCoeffs &coeffs_of, int64_t 
                        double smin, double smax, double *X, int64_t k, const PolishDone &done,
                        const PolishNeeds &needs, int64_t max_passes, FilterCount &fc,
                        int64_t *qr_fallbacks, const std::vector<double> &lam0,
-                       const std::vector<double> &res0, bool filter_all, bool verbose,
-                       const PolishTrace &trace) {
+                       const std::vector<double> &res0, double emin, double emax,
+                       bool filter_all, bool verbose, const PolishTrace &trace) {
   PolishOut out;
   sma_ctx *ctx = op->ctx;
   cudaStream_t st = ctx->stream;
@@ -240,23 +240,51 @@ PolishOut polish_mixed(const sma_op *op, const PolishCoeffs &coeffs_of, int64_t 
   // Rayleigh-Ritz.  The columns of V (filtered candidates and Ritz vectors of the basis)
   // are nearly orthogonal, so S is well conditioned; when it is not positive definite the
   // orthonormalizing path runs instead.
-  DevBuf<double> S;
+  // Both products are symmetric, so only their upper triangles are formed.  The Ritz
+  // vectors with values in [emin, emax] are lifted first (columns 0..kin-1 of X); the
+  // others only when done() says the polish goes on.
+  DevBuf<double> S, E;
+  DevBuf<int64_t> perm_d;
   auto rayleigh_ritz_gen = [&](double *V) {
-    if (!S.p) S.alloc(k * k, st);
+    if (!S.p) {
+      S.alloc(k * k, st);
+      E.alloc(k * k, st);
+      perm_d.alloc(k, st);
+    }
     op_apply(op, st, V, k, AX.p, k, k);
-    dn.gram(n, k, k, V, k, V, k, S.p, k);
-    dn.gram(n, k, k, V, k, AX.p, k, H.p, k);
+    dn.gram(n, k, k, V, k, V, k, S.p, k, 1.0, 0.0, true);
+    dn.gram(n, k, k, V, k, AX.p, k, H.p, k, 1.0, 0.0, true);
     if (!dn.sygvd(k, H.p, k, S.p, k, mu.p)) {
       if (qr_fallbacks) ++*qr_fallbacks;
       rayleigh_ritz(V);
       return;
     }
-    dn.mul_small(n, k, k, V, k, H.p, k, X, k, 1.0, 0.0);
-    op_apply(op, st, X, k, AX.p, k, k);
-    column_reduce(st, 0, n, k, X, k, AX.p, k, nullptr, lam_d.p, scratch);
-    column_reduce(st, 1, n, k, X, k, AX.p, k, lam_d.p, res_d.p, scratch);
-    out.lam = dev_to_host(st, lam_d.p, k);
-    out.res = dev_to_host(st, res_d.p, k);
+    const std::vector<double> muh = dev_to_host(st, mu.p, k);
+    std::vector<int64_t> perm;
+    for (int64_t j = 0; j < k; ++j)
+      if (emin <= muh[j] && muh[j] <= emax) perm.push_back(j);
+    const int64_t kin = (int64_t)perm.size();
+    for (int64_t j = 0; j < k; ++j)
+      if (!(emin <= muh[j] && muh[j] <= emax)) perm.push_back(j);
+    SMA_CUDA(cudaMemcpyAsync(perm_d.p, perm.data(), k * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    launch_gather_columns_cm(st, k, k, H.p, k, perm_d.p, E.p, k);
+    SMA_CUDA(cudaStreamSynchronize(st));  // perm must outlive its copy
+    out.lam.assign(k, 0.0);
+    out.res.assign(k, INFINITY);
+    for (int64_t j = kin; j < k; ++j) out.lam[j] = muh[perm[j]];
+    auto lift = [&](int64_t c0, int64_t c1) {  // Ritz vectors c0..c1-1 (perm order) into X
+      const int64_t c = c1 - c0;
+      if (c <= 0) return;
+      dn.mul_small(n, k, c, V, k, E.p + c0 * k, k, X + c0, k, 1.0, 0.0);
+      op_apply(op, st, X + c0, k, AX.p + c0, k, c);
+      column_reduce(st, 0, n, c, X + c0, k, AX.p + c0, k, nullptr, lam_d.p, scratch);
+      column_reduce(st, 1, n, c, X + c0, k, AX.p + c0, k, lam_d.p, res_d.p, scratch);
+      const std::vector<double> l = dev_to_host(st, lam_d.p, c), r = dev_to_host(st, res_d.p, c);
+      std::copy(l.begin(), l.end(), out.lam.begin() + c0);
+      std::copy(r.begin(), r.end(), out.res.begin() + c0);
+    };
+    lift(0, kin);
+    if (!done(out.lam, out.res)) lift(kin, k);
   };
   // phase times for the verbose trace (the stream is synchronized only then)
   auto now_ms = [&]() {

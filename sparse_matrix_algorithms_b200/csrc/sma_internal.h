@@ -347,10 +347,11 @@ void dgemm_update(cudaStream_t st, int num_sms, int64_t n, int64_t m, int64_t p,
                   int64_t ldx, const double *C, int64_t ldc, bool transC, double *Y, int64_t ldy,
                   double alpha, double beta);
 // C (m x k, column-major, ldc) = alpha X^T Y + beta C; deterministic split-n reduction
-// through `work` (grown as needed).
+// through `work` (grown as needed).  upper (m == k): only the 64 x 64 tiles on and above
+// the diagonal are computed and written -- the upper triangle of a symmetric product.
 void dgemm_gram(cudaStream_t st, int num_sms, int64_t n, int64_t m, int64_t k, const double *X,
                 int64_t ldx, const double *Y, int64_t ldy, double *C, int64_t ldc, double alpha,
-                double beta, DevBuf<double> &work);
+                double beta, DevBuf<double> &work, bool upper = false);
 
 struct Dense {
   sma_ctx *ctx;
@@ -358,16 +359,17 @@ struct Dense {
   explicit Dense(sma_ctx *c) : ctx(c) {}
   // C (col-major, m x k, ldc) = alpha * X^T Y + beta*C, X row-major n x m (ldx), Y n x k
   void gram(int64_t n, int64_t m, int64_t k, const double *X, int64_t ldx, const double *Y,
-            int64_t ldy, double *C, int64_t ldc, double alpha = 1.0, double beta = 0.0);
+            int64_t ldy, double *C, int64_t ldc, double alpha = 1.0, double beta = 0.0,
+            bool upper = false);
   // Y (row-major n x p, ldy) = alpha * X C + beta*Y, X row-major n x m, C col-major m x p
   void mul_small(int64_t n, int64_t m, int64_t p, const double *X, int64_t ldx, const double *C,
                  int64_t ldc, double *Y, int64_t ldy, double alpha, double beta, bool transC = false);
   // Symmetric eigen-decomposition of a k x k column-major matrix in place (vectors
   // overwrite A, eigenvalues ascending in w_dev). uplo_upper selects the triangle read.
   void syevd(int64_t k, double *A, int64_t lda, double *w_dev, bool uplo_upper);
-  // Generalized symmetric-definite eigenproblem A E = B E diag(w) (k x k column-major, lower
-  // triangles read): E overwrites A (B-orthonormal), B its Cholesky factor, eigenvalues
-  // ascending in w_dev.  Returns false when B is not positive definite.
+  // Generalized symmetric-definite eigenproblem A E = B E diag(w) (k x k column-major, the
+  // upper triangles read): E overwrites A (B-orthonormal), B its Cholesky factor,
+  // eigenvalues ascending in w_dev.  Returns false when B is not positive definite.
   bool sygvd(int64_t k, double *A, int64_t lda, double *B, int64_t ldb, double *w_dev);
 };
 
@@ -389,7 +391,7 @@ FilterCount percol_filter(const sma_op *op, cudaStream_t st, const T *coef, int6
 // e[0..K-1]: Chebyshev coefficients of (p(s) - p(t)) / (s - t) for p = sum c_m T_m; *pt = p(t).
 void divided_difference(const std::vector<double> &c, double t, double *e, double *pt);
 struct PolishOut {
-  std::vector<double> lam, res;  // Ritz values (ascending) and residual norms of X
+  std::vector<double> lam, res;  // Ritz values and residual norms of X's columns
   int64_t passes = 0;
   int64_t columns = 0;  // columns filtered, summed over the passes
   int64_t degree = 0;   // polish degree of the last pass
@@ -426,14 +428,17 @@ PolishConfig polish_config();
 // Rayleigh-Ritz with A on all k columns; X ends as the last Ritz vectors.
 // lam0/res0: each column's Rayleigh quotient and residual norm on entry (its columns unit
 // vectors); when empty (or with filter_all), a Rayleigh-Ritz of the k columns comes first.
+// Without filter_all, each Rayleigh-Ritz lifts the Ritz vectors with values in [emin, emax]
+// first and the others only when done() is false; after a pass that ends the polish, the
+// columns past the in-window ones are not lifted (their lam is the Ritz value, res inf).
 // The degree starts at K0; after a pass (other than the first) that cut the worst unconverged
 // residual by less than 3x the next pass doubles it, up to Kmax.
 PolishOut polish_mixed(const sma_op *op, const PolishCoeffs &coeffs_of, int64_t K0, int64_t Kmax,
                        double smin, double smax, double *X, int64_t k, const PolishDone &done,
                        const PolishNeeds &needs, int64_t max_passes, FilterCount &fc,
                        int64_t *qr_fallbacks, const std::vector<double> &lam0,
-                       const std::vector<double> &res0, bool filter_all, bool verbose,
-                       const PolishTrace &trace = PolishTrace());
+                       const std::vector<double> &res0, double emin, double emax,
+                       bool filter_all, bool verbose, const PolishTrace &trace = PolishTrace());
 
 // ------------------------------------------------------------------ result
 }  // namespace sma
