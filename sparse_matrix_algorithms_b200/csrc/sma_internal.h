@@ -72,6 +72,7 @@ struct CsrTune {
   std::vector<int> cands;           // encoded candidate configurations
   std::vector<int> trial;           // configuration of each timed launch so far
   std::vector<cudaEvent_t> events;  // start/stop event pair per timed launch
+  int round = 0;                    // 0: every candidate twice; 1: the four best again
   int chosen = -1;                  // encoded winner once decided
   CsrTune() = default;
   CsrTune(const CsrTune &) = delete;
