@@ -739,6 +739,67 @@ def run_profile_pipeline(args):
                                             "kernel_launches") if k in st}}), flush=True)
 
 
+def run_profile_dense(args):
+    """This library's DMMA products (sma_dense_gram_dev, sma_dense_update_dev) against
+    torch.matmul in float64 (cuBLAS) at the tall-skinny shapes of a C3 POLFED solve
+    (n = 262144): the CholQR2 products (64 x 64), the reorthogonalization against a basis
+    of 2048 columns, the polish's Rayleigh-Ritz (1976 x 1976) and the Ritz-vector lift
+    (3904 -> 3000).  Best of 4 timed runs after one warm-up, CUDA events."""
+    import torch
+
+    import sparse_matrix_algorithms_b200 as S
+    from sparse_matrix_algorithms_b200 import _lib as L
+
+    ctx = S.context(0)
+    lib = L.load()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    n = 262144
+    shapes = [("gram", 64, 64), ("update", 64, 64), ("gram", 2048, 64), ("update", 2048, 64),
+              ("gram", 1976, 1976), ("update", 1976, 1976), ("update", 3904, 3000)]
+
+    def timeit(fn, s=None):
+        ts = []
+        for _ in range(5):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            fn()
+            e1.record(s)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return min(ts[1:])
+
+    for kind, m, k in shapes:
+        X = torch.randn(n, m, dtype=torch.float64, device="cuda")
+        if kind == "gram":  # C (m x k, column-major) = X^T Y
+            Y = torch.randn(n, k, dtype=torch.float64, device="cuda")
+            C = torch.empty(k, m, dtype=torch.float64, device="cuda")
+
+            def ours():
+                L.check(lib.sma_dense_gram_dev(ctx.handle, n, m, k, X.data_ptr(), m, Y.data_ptr(),
+                                               k, C.data_ptr(), m, 1.0, 0.0))
+
+            def ref():
+                torch.matmul(X.T, Y)
+        else:  # Y (n x k) = X B, B column-major m x k
+            B = torch.randn(k, m, dtype=torch.float64, device="cuda")
+            Y = torch.empty(n, k, dtype=torch.float64, device="cuda")
+
+            def ours():
+                L.check(lib.sma_dense_update_dev(ctx.handle, n, m, k, X.data_ptr(), m, B.data_ptr(),
+                                                 m, 0, Y.data_ptr(), k, 1.0, 0.0))
+
+            def ref():
+                torch.matmul(X, B.T)
+        flops = 2.0 * n * m * k
+        t_ours, t_ref = timeit(ours, stream), timeit(ref)
+        print(json.dumps({"profile_dense": kind, "n": n, "m": m, "k": k, "ms": round(t_ours, 3),
+                          "tflops": round(flops / t_ours / 1e9, 1), "cublas_ms": round(t_ref, 3),
+                          "cublas_tflops": round(flops / t_ref / 1e9, 1)}), flush=True)
+        del X, Y
+        torch.cuda.empty_cache()
+
+
 def run_profile_slice(args):
     """One iteration of batched slicing on the C3 matrix: four windows around E=0 with
     degrees 400/300/200/100 and widths 256/192/192/128 (768 columns at the top degree),
@@ -778,6 +839,8 @@ def main():
                     help="a short C3 POLFED solve for ncu captures of its GEMMs")
     ap.add_argument("--profile-pipeline", action="store_true",
                     help="one pipeline solve of the workload (for ncu launch lists)")
+    ap.add_argument("--profile-dense", action="store_true",
+                    help="this library's DMMA products against cuBLAS at the solver's shapes")
     ap.add_argument("--profile-slice", action="store_true",
                     help="one batched slicing iteration on the C3 matrix for ncu captures")
     ap.add_argument("--width", type=int, default=0, help="block width (default: the workload's s)")
@@ -792,6 +855,9 @@ def main():
         return
     if args.profile_pipeline:
         run_profile_pipeline(args)
+        return
+    if args.profile_dense:
+        run_profile_dense(args)
         return
     if args.profile_slice:
         run_profile_slice(args)
