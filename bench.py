@@ -822,6 +822,38 @@ def run_profile_dense(args):
         torch.cuda.empty_cache()
 
 
+def run_profile_stream(args):
+    """The HBM rate of plain streams with the fused step's traffic mix, as a practical
+    ceiling beside the copy peak: torch elementwise kernels over FP32 blocks of the C3
+    step's size (n = 262144 rows x 64 columns = 67 MB each, and x 768 = 805 MB):
+    copy (1 read + 1 write), add (2 + 1) and addcmul (3 reads + 1 write, the step's Q, B1,
+    B2 -> out).  Best of 10 after warm-up, CUDA events."""
+    import torch
+
+    n = 262144
+    for cols in (64, 768):
+        a, b, c, d = (torch.randn(n, cols, device="cuda") for _ in range(4))
+        blk = a.numel() * 4
+        for name, fn, nbytes in (("copy", lambda: d.copy_(a), 2 * blk),
+                                 ("add", lambda: torch.add(a, b, out=d), 3 * blk),
+                                 ("addcmul", lambda: torch.addcmul(a, b, c, out=d), 4 * blk)):
+            for _ in range(3):
+                fn()
+            ts = []
+            for _ in range(10):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                fn()
+                e1.record()
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            t = min(ts)
+            print(json.dumps({"profile_stream": name, "block_mb": round(blk / 1e6, 1),
+                              "us": round(1e3 * t, 1), "gbs": round(nbytes / t / 1e6, 1)}), flush=True)
+        del a, b, c, d
+        torch.cuda.empty_cache()
+
+
 def run_profile_slice(args):
     """One iteration of batched slicing on the C3 matrix: four windows around E=0 with
     degrees 400/300/200/100 and widths 256/192/192/128 (768 columns at the top degree),
@@ -863,6 +895,8 @@ def main():
                     help="one pipeline solve of the workload (for ncu launch lists)")
     ap.add_argument("--profile-dense", action="store_true",
                     help="this library's DMMA products against cuBLAS at the solver's shapes")
+    ap.add_argument("--profile-stream", action="store_true",
+                    help="HBM rate of plain elementwise streams with the step's traffic mix")
     ap.add_argument("--profile-slice", action="store_true",
                     help="one batched slicing iteration on the C3 matrix for ncu captures")
     ap.add_argument("--width", type=int, default=0, help="block width (default: the workload's s)")
@@ -880,6 +914,9 @@ def main():
         return
     if args.profile_dense:
         run_profile_dense(args)
+        return
+    if args.profile_stream:
+        run_profile_stream(args)
         return
     if args.profile_slice:
         run_profile_slice(args)
