@@ -108,6 +108,8 @@ int sma_ctx_create(int device, sma_ctx **out) {
     ctx->persistent = pe && std::string(pe) == "1";
     const char *cd = std::getenv("SMA_CUBLAS_DENSE");
     ctx->cublas_dense = cd && std::string(cd) == "1";
+    const char *pd = std::getenv("SMA_PDL");
+    ctx->pdl = !(pd && std::string(pd) == "0");
     try {
       SMA_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
       SMA_CUBLAS(cublasCreate(&ctx->cublas));

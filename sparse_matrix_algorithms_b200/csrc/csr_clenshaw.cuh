@@ -13,6 +13,12 @@
 //           addresses, which the L1 cache serves as one broadcast;
 //   STAGED  the CTA first copies the pairs of all its rows (one contiguous CSR range)
 //           into shared memory with coalesced loads, then reads them from there.
+// Both families are launched as programmatic dependents of the previous step (when the
+// context allows it): a CTA first lets the next step's grid be scheduled, reads what no
+// step writes (its CSR rows and the row of Q), and only then waits for the previous grid
+// to complete (griddepcontrol.wait) before it reads B1 or B2 or writes anything -- so the
+// next step's CTAs fill the SMs that this step's last wave leaves idle.  Launched without
+// the attribute, both instructions are no-ops.
 // Every configuration accumulates with FMA in ascending column order -- the order of the
 // reference's CSC product on a symmetric matrix -- so all configurations write
 // bit-identical results, and the autotuner may run real recurrence steps with different
@@ -97,6 +103,11 @@ __device__ __forceinline__ void row_product(const int *__restrict__ cols, const 
   }
 }
 
+// Programmatic dependent launch: let the next grid in the stream be scheduled; wait until
+// the grids this one depends on have completed and their writes are visible.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 template <typename T, int V, int G, int U, bool HQ, bool HS, bool HB, bool PC>
 __global__ void __launch_bounds__(kThreads)
 direct_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
@@ -105,16 +116,24 @@ direct_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
               T *__restrict__ out, int64_t ldo, T ck, T alpha, T beta,
               const T *__restrict__ cseg, const int *__restrict__ colseg) {
   constexpr int kRows = kThreads / G;
+  pdl_trigger();
   const int64_t row = (int64_t)blockIdx.x * kRows + threadIdx.x / G;
-  if (row >= n) return;
+  const bool live = row < n;
   const int lane = threadIdx.x % G;
-  const int start = __ldg(rowptr + row);
-  const int end = __ldg(rowptr + row + 1);
+  int start = 0, end = 0;
+  T q[V], s[V], t[V];
+  if (live) {  // what no step writes: the CSR row and the first pass's row of Q
+    start = __ldg(rowptr + row);
+    end = __ldg(rowptr + row + 1);
+    if constexpr (HQ) if (lane * V < b) ldv<T, V>(Q + row * ldq + lane * V, q);
+  }
+  pdl_wait();
+  if (!live) return;
   for (int c0 = lane * V; c0 < b; c0 += G * V) {
-    T q[V], s[V], t[V], acc[V];
+    T acc[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) acc[v] = T(0);
-    if constexpr (HQ) ldv<T, V>(Q + row * ldq + c0, q);
+    if constexpr (HQ) if (c0 != lane * V) ldv<T, V>(Q + row * ldq + c0, q);
     if constexpr (HS) ldv<T, V>(B1 + row * ldb + c0, s);
     if constexpr (HB) ldv<T, V>(B2 + row * ldb + c0, t);
     row_product<T, V, U>(colind, val, 0, start, end, B1 + c0, ldb, acc);
@@ -134,7 +153,13 @@ staged_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
   constexpr int kRows = kThreads / G;
   __shared__ int s_col[kStage];
   __shared__ T s_val[kStage];
+  pdl_trigger();
   const int64_t row0 = (int64_t)blockIdx.x * kRows;
+  const int64_t row = row0 + threadIdx.x / G;
+  const int lane = threadIdx.x % G;
+  const bool live = row < n;
+  T q[V], s[V], t[V];
+  if constexpr (HQ) if (live && lane * V < b) ldv<T, V>(Q + row * ldq + lane * V, q);
   const int64_t rlast = min(n, row0 + kRows);
   const int base = __ldg(rowptr + row0);
   const int top = __ldg(rowptr + rlast);
@@ -146,16 +171,15 @@ staged_kernel(const int *__restrict__ rowptr, const int *__restrict__ colind,
     }
   }
   __syncthreads();
-  const int64_t row = row0 + threadIdx.x / G;
-  if (row >= n) return;  // no barrier follows
-  const int lane = threadIdx.x % G;
+  pdl_wait();  // B1 and B2 come from the previous steps
+  if (!live) return;  // no barrier follows
   const int start = __ldg(rowptr + row);
   const int end = __ldg(rowptr + row + 1);
   for (int c0 = lane * V; c0 < b; c0 += G * V) {
-    T q[V], s[V], t[V], acc[V];
+    T acc[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) acc[v] = T(0);
-    if constexpr (HQ) ldv<T, V>(Q + row * ldq + c0, q);
+    if constexpr (HQ) if (c0 != lane * V) ldv<T, V>(Q + row * ldq + c0, q);
     if constexpr (HS) ldv<T, V>(B1 + row * ldb + c0, s);
     if constexpr (HB) ldv<T, V>(B2 + row * ldb + c0, t);
     if (staged) row_product<T, V, U>(s_col, s_val, base, start, end, B1 + c0, ldb, acc);
@@ -395,6 +419,26 @@ struct Args {
   const int *colseg = nullptr;
 };
 
+// Launch of a DIRECT or STAGED step: as a programmatic dependent of the previous launch in
+// the stream when the context allows it (the kernels wait for their predecessor before
+// they touch B1, B2 or the output), else an ordinary launch.
+template <typename... KArgs, typename... Args>
+void launch_step(const sma_op *op, void (*kernel)(KArgs...), unsigned grid, cudaStream_t st,
+                 Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = op->ctx->pdl ? 1 : 0;
+  SMA_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+  SMA_CHECK_LAUNCH();
+}
+
 template <typename T, int V, int G, int U, bool HQ, bool HS, bool HB>
 void launch_one(int fam, const Args<T> &a) {
   const T *val;
@@ -402,30 +446,22 @@ void launch_one(int fam, const Args<T> &a) {
   else val = (const T *)a.op->val32;
   constexpr int kRows = kThreads / G;
   const unsigned grid = (unsigned)((a.op->n + kRows - 1) / kRows);
+  const sma_op *op = a.op;
   if constexpr (HQ && HS && HB) {
     if (a.cseg) {
-      if (fam == 0)
-        direct_kernel<T, V, G, U, true, true, true, true><<<grid, kThreads, 0, a.st>>>(
-            a.op->rowptr, a.op->colind, val, a.op->n, (int)a.b, a.Q, a.ldq, a.B1, a.B2, a.ldb,
-            a.out, a.ldo, T(0), (T)a.alpha, (T)a.beta, a.cseg, a.colseg);
-      else
-        staged_kernel<T, V, G, U, true, true, true, true><<<grid, kThreads, 0, a.st>>>(
-            a.op->rowptr, a.op->colind, val, a.op->n, (int)a.b, a.Q, a.ldq, a.B1, a.B2, a.ldb,
-            a.out, a.ldo, T(0), (T)a.alpha, (T)a.beta, a.cseg, a.colseg);
-      SMA_CHECK_LAUNCH();
-      return;
+      auto k = fam == 0 ? direct_kernel<T, V, G, U, true, true, true, true>
+                        : staged_kernel<T, V, G, U, true, true, true, true>;
+      return launch_step(op, k, grid, a.st, op->rowptr, op->colind, val, op->n, (int)a.b, a.Q,
+                         a.ldq, a.B1, a.B2, a.ldb, a.out, a.ldo, T(0), (T)a.alpha, (T)a.beta,
+                         a.cseg, a.colseg);
     }
   }
   if (a.cseg) throw Error(SMA_ERR_INTERNAL, "segmented Clenshaw step needs the full variant");
-  if (fam == 0)
-    direct_kernel<T, V, G, U, HQ, HS, HB, false><<<grid, kThreads, 0, a.st>>>(
-        a.op->rowptr, a.op->colind, val, a.op->n, (int)a.b, a.Q, a.ldq, a.B1, a.B2, a.ldb, a.out,
-        a.ldo, (T)a.ck, (T)a.alpha, (T)a.beta, nullptr, nullptr);
-  else
-    staged_kernel<T, V, G, U, HQ, HS, HB, false><<<grid, kThreads, 0, a.st>>>(
-        a.op->rowptr, a.op->colind, val, a.op->n, (int)a.b, a.Q, a.ldq, a.B1, a.B2, a.ldb, a.out,
-        a.ldo, (T)a.ck, (T)a.alpha, (T)a.beta, nullptr, nullptr);
-  SMA_CHECK_LAUNCH();
+  auto k = fam == 0 ? direct_kernel<T, V, G, U, HQ, HS, HB, false>
+                    : staged_kernel<T, V, G, U, HQ, HS, HB, false>;
+  launch_step(op, k, grid, a.st, op->rowptr, op->colind, val, op->n, (int)a.b, a.Q, a.ldq, a.B1,
+              a.B2, a.ldb, a.out, a.ldo, (T)a.ck, (T)a.alpha, (T)a.beta, (const T *)nullptr,
+              (const int *)nullptr);
 }
 
 template <typename T, int G, int NB, bool HQ, bool HS, bool HB>

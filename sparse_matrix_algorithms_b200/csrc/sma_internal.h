@@ -102,6 +102,9 @@ struct sma_ctx {
   // SMA_CUBLAS_DENSE=1: the tall-skinny products go through cuBLAS DGEMM instead of this
   // library's DMMA kernels (dgemm.cu) -- for comparisons
   bool cublas_dense = false;
+  // SMA_PDL=0 turns off programmatic dependent launch of the fused CSR steps (the next
+  // step's CTAs start on SMs the previous step's last wave leaves idle)
+  bool pdl = true;
 };
 
 // OP_CSR_HALF: the upper triangle of a symmetric matrix only (half.cu)
