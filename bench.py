@@ -563,6 +563,9 @@ def run_ours(args, rank, world, device):
 TRAFFIC = {
     ("c2", "fp64"): 43_698_688 + 242_944,
     ("c3", "fp64"): 429_926_656 + 117_963_264,
+    # the MIXED pipeline's basis filter: the FP32 b=64 step (profiles/clenshaw_step_anderson_L64_b64_fp32.md)
+    ("c3", "mixed"): 219_189_760 + 50_311_424,
+    ("c3", "fp32"): 219_189_760 + 50_311_424,
 }
 
 
