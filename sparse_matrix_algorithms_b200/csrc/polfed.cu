@@ -288,7 +288,7 @@ class PolfedWindow {
     // MIXED with unfiltered guards: the polish's Rayleigh-Ritz (on the candidates, filtered,
     // and the guards) takes the place of the refinement, which would only rotate the
     // candidates among themselves first
-    if (o.refine && !(o.precision == SMA_PREC_MIXED && !pc.filter_guards)) {
+    if (o.refine && !(o.precision == SMA_PREC_MIXED && !pc.filter_guards && !pc.refine)) {
       // refine_original_rr (polfed.jl:837-880); orth_block_polfed! at its default rtol=1e-12
       const int64_t k = orthonormalize(ctx_, n, npre, Xc_.p, npre, true, 1e-12, nullptr, &stats.qr_fallbacks);
       if (k == 0) return empty();

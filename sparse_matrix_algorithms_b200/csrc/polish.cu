@@ -177,6 +177,7 @@ PolishConfig polish_config() {
   if (const char *d = std::getenv("SMA_POLISH_DEGREE")) c.degree_scale = std::max(0.05, std::atof(d));
   if (const char *p = std::getenv("SMA_POLISH_PASSES")) c.max_passes = std::max(0, std::atoi(p));
   if (const char *v = std::getenv("SMA_POLISH_VERBOSE")) c.verbose = std::string(v) == "1";
+  if (const char *r = std::getenv("SMA_POLISH_REFINE")) c.refine = std::string(r) == "1";
   return c;
 }
 

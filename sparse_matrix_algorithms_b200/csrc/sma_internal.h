@@ -423,6 +423,7 @@ struct PolishConfig {
   double degree_scale = 1.0;
   int64_t max_passes = 5;
   bool verbose = false;
+  bool refine = false;  // SMA_POLISH_REFINE=1: keep the refinement before the polish
 };
 PolishConfig polish_config();
 // Up to max_passes filtered subspace iterations on the k columns of X (n x k, ld k, FP64,
