@@ -363,6 +363,35 @@ def test_polfed_mixed_precision_xxz(lib_built):
     assert res.max() <= 1e-10 * nrm
 
 
+@pytest.mark.parametrize("env", [{"SMA_POLISH_FILTER_GUARDS": "1"},
+                                 {"SMA_POLISH_REFINE": "1"},
+                                 {"SMA_POLISH_FILTER": "step", "SMA_POLISH_GUARDS": "2"}])
+def test_polfed_mixed_polish_variants(lib_built, monkeypatch, env):
+    """The polish's alternative settings (filtered guards with a Rayleigh-Ritz first, the
+    refinement kept, an undamped step polynomial over the guards' span with fewer guards)
+    reach the same pairs as the default: the exact count, |dlambda| <= 1e-12 ||A||, relative
+    residual <= 1e-10, and residuals that match the returned vectors."""
+    import sparse_matrix_algorithms_b200 as S
+
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    A = M.xxz_sz0(12, 5.0, 1)
+    lam_all = np.linalg.eigvalsh(A.toarray())
+    nrm = _norm2(lam_all)
+    mid = int(np.argmin(np.abs(lam_all - 0.5 * (lam_all[0] + lam_all[-1]))))
+    emin, emax = _window_with_gaps(lam_all, mid - 10, mid + 9)
+    smin, smax = O.gershgorin_bounds(A)
+    st = {}
+    lam, X, res = S.polfed(A, 20, 800, s=8, smin=smin, smax=smax, sigma=0.5 * (emin + emax),
+                           emin=emin, emax=emax, mmax=10, precision="mixed", stats=st)
+    assert st["polish_iterations"] >= 1
+    assert lam.size == 20
+    assert np.abs(np.sort(lam) - lam_all[mid - 10:mid + 10]).max() <= 1e-12 * nrm
+    assert res.max() <= 1e-10 * nrm
+    r = np.linalg.norm(A @ X - X * lam, axis=0)
+    assert np.abs(r - res).max() <= 1e-12 * nrm
+
+
 def test_filter_graph_replay_is_bit_identical(lib_built, monkeypatch):
     """POLFED calls the same filter once per block: from the second call the recurrence is
     replayed from a CUDA graph.  A context with graphs off gives bit-identical results."""
